@@ -1,0 +1,330 @@
+"""Benchmark of the fused sm_100a time step (contract: one JSON line on rank 0).
+
+Default workload: SlitConfig (free-slip plates confining x) 64x256x256,
+params.h defaults with zeta (ALPHA) = 0.01, centred advection, FP32 compute
+with populations stored as FP32 deviations, seeded random-director initial
+condition.  A "step" is one full time step (Q-tensor update + body force +
+D3Q15 collide/stream) over the whole box.
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl reference]
+                    [--workload slit64|channel20|periodic512|periodic32]
+                    [--precision fp32|fp64|fp16]
+
+value    : MLUPS (million lattice-cell updates per second), all GPUs, device
+           resident fields, timed with CUDA events on the solver's stream,
+           max over ranks.
+e2e      : the same metric through the C ABI with host (pinned) buffers: each
+           e2e step uploads rho/u/Q, runs kSaveInterval = 100 solver steps and
+           downloads rho/u/Q, as ActiveNematicSim's save cycle does.
+roofline : algorithmic bytes per cell update (f 15+15, Q 5+5, u 3+3 words;
+           184 B in FP32) x cells / average fused-kernel duration, against the
+           measured HBM copy bandwidth.
+--impl reference : the reference's own OpenMP CPU solver (oracle/_ref build
+           of its sources) on this machine's host cores, bounded sample.
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import statistics
+import subprocess
+import sys
+import tempfile
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+WORKLOADS = {
+    # name: (nx, ny, nz, bc, ALPHA, ref_build)
+    "slit64": (64, 256, 256, "slit", 0.01, "b_slit"),
+    "channel20": (20, 100, 100, "channel", 0.01, "b_channel"),
+    "periodic512": (512, 512, 512, "periodic", 0.01, None),
+    "periodic32": (32, 32, 32, "periodic", 0.023, "b_p32"),
+}
+BYTES_PER_CELL = {"fp64": 368, "fp32": 184, "fp16": 124}
+
+
+def measured_peaks():
+    p = os.path.join(ROOT, "MEASURED_PEAKS.json")
+    if os.path.exists(p):
+        with open(p) as fh:
+            d = json.load(fh)
+        return float(d["hbm_gbs"]), "measured"
+    return 6650.0, "fallback"
+
+
+def profile_traffic(workload, precision):
+    """DRAM bytes per fused-step launch from the committed ncu summary, or None."""
+    path = os.path.join(ROOT, "profiles", f"fused_step_{workload}_{precision}.md")
+    if not os.path.exists(path):
+        return None
+    for line in open(path):
+        if line.strip().startswith("traffic_bytes_per_launch:"):
+            try:
+                return float(line.split(":", 1)[1].strip())
+            except ValueError:
+                return None
+    return None
+
+
+def bc_for(name):
+    import lbman3d_b200 as L
+    return {"slit": L.SlitConfig, "channel": L.ChannelConfig, "periodic": L.FullyPeriodicConfig}[name]()
+
+
+class ClockSampler:
+    """nvidia-smi samples of SM clock and throttle reasons during the timed region."""
+    Q = ("clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,clocks_event_reasons.hw_slowdown,"
+         "clocks_event_reasons.hw_thermal_slowdown,clocks_event_reasons.sw_thermal_slowdown,"
+         "clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, device):
+        self.device, self.proc, self.out = device, None, None
+
+    def __enter__(self):
+        try:
+            self.out = tempfile.TemporaryFile(mode="w+")
+            self.proc = subprocess.Popen(["nvidia-smi", f"--query-gpu={self.Q}", "--format=csv,noheader,nounits",
+                                          "-lms", "100", "-i", str(self.device)], stdout=self.out,
+                                         stderr=subprocess.DEVNULL)
+            time.sleep(0.3)
+        except (OSError, FileNotFoundError):
+            self.proc = None
+        return self
+
+    def __exit__(self, *a):
+        if self.proc:
+            time.sleep(0.2)
+            self.proc.terminate()
+            self.proc.wait(timeout=10)
+
+    def summary(self):
+        if not self.proc:
+            return None
+        self.out.seek(0)
+        rows = [r.split(",") for r in self.out.read().strip().splitlines() if r.count(",") >= 7]
+        if not rows:
+            return None
+        sm = [float(r[0]) for r in rows if r[0].strip().replace(".", "").isdigit()]
+        mx = max(float(r[1]) for r in rows)
+        reasons = set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for r in rows:
+            for nm, v in zip(names, r[4:8]):
+                if v.strip().lower() == "active":
+                    reasons.add(nm)
+        return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": mx, "reasons": sorted(reasons),
+                "samples": len(rows)}
+
+
+def make_sim(workload, precision, device):
+    import lbman3d_b200 as L
+    nx, ny, nz, bc, alpha, _ = WORKLOADS[workload]
+    p = L.Params(nx=nx, ny=ny, nz=nz, ALPHA=alpha)
+    prec = {"fp64": L.Precision.FP64, "fp32": L.Precision.FP32, "fp16": L.Precision.FP16}[precision]
+    sim = L.Simulation(p, bc_for(bc), prec, device=device)
+    return sim, p
+
+
+def time_device(sim, steps, warmup, stream):
+    """Device-resident steps timed with CUDA events on the solver's stream."""
+    import torch
+    S0 = 0.5
+    sim.init_seeded(1234, S0, 1e-3)
+    sim.step(warmup)
+    sim.synchronize()
+    l0 = sim.launch_count()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record(stream)
+    sim.step(steps)
+    e1.record(stream)
+    e1.synchronize()
+    return e0.elapsed_time(e1), sim.launch_count() - l0
+
+
+def error_vs_fp64(workload, precision, device, nsteps=100):
+    """Per-field max relative error against the FP64 path (bitwise the
+    reference arithmetic) on the same seed after nsteps."""
+    a, _ = make_sim(workload, precision, device)
+    b, _ = make_sim(workload, "fp64", device)
+    for s in (a, b):
+        s.init_seeded(1234, 0.5, 1e-3)
+        s.step(nsteps)
+    x, y = a.download(), b.download()
+    a.close(), b.close()
+    out = {}
+    for f in ("rho", "u", "q"):
+        ref = y[f] - (1.0 if f == "rho" else 0.0)
+        out[f] = float(np.max(np.abs(x[f] - y[f])) / max(np.max(np.abs(ref)), 1e-300))
+    out["steps"] = nsteps
+    return out
+
+
+def time_e2e(sim, p, iters, stream, save_interval=100):
+    import torch
+    V = p.V
+    pin = lambda n: torch.empty(n, dtype=torch.float64, pin_memory=True).numpy()
+    rho, u, q = pin(V), pin(3 * V), pin(5 * V)
+    sim.init_seeded(99, 0.5, 1e-3)
+    out = sim.download()
+    rho[:], u[:], q[:] = out["rho"], out["u"], out["q"]
+    orho, ou, oq = pin(V), pin(3 * V), pin(5 * V)
+    from lbman3d_b200 import _native as N
+    lib, h = N.lib(), sim.handle
+
+    def cycle():
+        N.check(lib.lbman_upload(h, N.dptr(rho), N.dptr(u), N.dptr(q), None, None))
+        N.check(lib.lbman_step(h, save_interval))
+        N.check(lib.lbman_download(h, N.dptr(orho), N.dptr(ou), N.dptr(oq), None, None))
+
+    cycle()
+    torch.cuda.synchronize()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record(stream)
+    for _ in range(iters):
+        cycle()
+    e1.record(stream)
+    e1.synchronize()
+    ms = e0.elapsed_time(e1)
+    mlups = V * save_interval * iters / (ms * 1e3)
+    return {"value": mlups, "unit": "MLUPS", "h2d_bytes_per_step": 9 * V * 8, "d2h_bytes_per_step": 9 * V * 8,
+            "solver_steps_per_step": save_interval, "steps": iters}
+
+
+def reference_cpu(workload, max_steps, warmup):
+    """The reference's OpenMP CPU solver on the host cores (oracle/_ref)."""
+    from oracle import build_ref
+    from oracle import oracle as O
+    nx, ny, nz, bc, alpha, tag = WORKLOADS[workload]
+    exe = build_ref.driver_path(tag) if tag else None
+    cores = os.cpu_count() or 1
+    V = nx * ny * nz
+    sys.path.insert(0, os.path.join(ROOT, "tests", "golden"))
+    from cases import BC
+    op = O.make_params(nx, ny, nz, BC[bc], ALPHA=alpha)
+    q = O.seeded_q(op, 1234, O.equilibrium_order(op), 1e-3)
+    if exe and os.path.exists(exe):
+        with tempfile.TemporaryDirectory() as td:
+            fin = os.path.join(td, "in.bin")
+            with open(fin, "wb") as fh:
+                fh.write(np.int64(V).tobytes() + np.int32(0).tobytes() + np.int32(0).tobytes())
+                fh.write(np.ones(V).tobytes() + np.zeros(3 * V).tobytes() + q.tobytes())
+            r = subprocess.run([exe, "--bench", bc, fin, str(warmup), str(max_steps)], capture_output=True,
+                               text=True, env=dict(os.environ, LBMAN_REF_THREADS=str(cores), OMP_NUM_THREADS=str(cores)),
+                               check=True)
+            d = json.loads(r.stdout.strip().splitlines()[-1])
+        return {"value": d["mlups"], "unit": "MLUPS", "cores": d["threads"], "kind": "reference",
+                "sample": f"{max_steps} full time steps of the {nx}x{ny}x{nz} box after {warmup} warm-up "
+                          f"(reference CPU solver built from its sources, OpenMP)", "ms_step": d["ms_step"]}
+    # C restatement (single thread per call site of OpenMP in the port)
+    sim = O.OracleSim(op)
+    sim.set(np.ones(V), np.zeros(3 * V), q)
+    sim.step(warmup)
+    t0 = time.perf_counter()
+    sim.step(max_steps)
+    dt = time.perf_counter() - t0
+    return {"value": V * max_steps / dt / 1e6, "unit": "MLUPS", "cores": cores, "kind": "port",
+            "sample": f"{max_steps} full time steps of the {nx}x{ny}x{nz} box (C restatement)",
+            "ms_step": dt * 1e3 / max_steps}
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=10000)
+    ap.add_argument("--warmup", type=int, default=50)
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--workload", default="slit64", choices=list(WORKLOADS))
+    ap.add_argument("--precision", default="fp32", choices=["fp32", "fp64", "fp16"])
+    ap.add_argument("--no-extras", action="store_true", help="skip e2e, cpu baseline and variants")
+    a = ap.parse_args()
+
+    rank = int(os.environ.get("RANK", "0"))
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    nx, ny, nz, bc, alpha, _ = WORKLOADS[a.workload]
+    V = nx * ny * nz
+    config = {"workload": f"{bc}_{nx}x{ny}x{nz}", "bc": bc, "zeta": alpha, "advection": "centred",
+              "init": "seeded random director, S0=0.5, 1e-3 Gaussian", "l2": "state larger than L2 (126 MB)"
+              if V * BYTES_PER_CELL[a.precision] > 126e6 else "state fits in L2", "parallelism": f"replicas x{a.gpus}"}
+
+    if a.impl == "reference":
+        if rank != 0:
+            return
+        n = max(1, min(a.steps, 20 if V > 1e6 else 200))
+        r = reference_cpu(a.workload, n, min(a.warmup, 2))
+        line = {"impl": "reference", "metric": "MLUPS", "value": r["value"], "unit": "MLUPS", "n_gpus": a.gpus,
+                "steps": n, "warmup": min(a.warmup, 2), "ms_per_step": r["ms_step"], "higher_is_better": True,
+                "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic", "config": config,
+                "cpu_baseline": {k: r[k] for k in ("value", "unit", "cores", "kind", "sample")},
+                "e2e": {"value": r["value"], "unit": "MLUPS", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+        print(json.dumps(line), flush=True)
+        return
+
+    import torch
+    import torch.distributed as dist
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    if world > 1:
+        dist.init_process_group("nccl", init_method="env://")
+    torch.cuda.set_device(local)
+    stream = torch.cuda.Stream(device=local)
+
+    sim, p = make_sim(a.workload, a.precision, local)
+    sim.set_stream(stream.cuda_stream)
+    if world > 1:
+        dist.barrier()
+    torch.cuda.synchronize()
+    with ClockSampler(local) as clk:
+        ms, launches = time_device(sim, a.steps, max(a.warmup, 3), stream)
+    if world > 1:
+        t = torch.tensor([ms], device="cuda")
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        ms = float(t.item())
+    ms_step = ms / a.steps
+    mlups = world * V * a.steps / (ms * 1e3)
+    peak, peak_kind = measured_peaks()
+    bpc = BYTES_PER_CELL[a.precision]
+    achieved = bpc * V / (ms_step * 1e-3) / 1e9
+    traffic = profile_traffic(config["workload"], a.precision)
+    line = {"metric": "MLUPS", "value": mlups, "unit": "MLUPS", "n_gpus": world, "steps": a.steps,
+            "warmup": max(a.warmup, 3), "ms_per_step": ms_step, "higher_is_better": True, "scaling": "weak",
+            "vs_baseline": None, "dtype": {"fp32": "f32", "fp64": "f64", "fp16": "f32 (f16 storage)"}[a.precision],
+            "data": "synthetic", "config": config, "gpu_launches": launches,
+            "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
+                         "frac": achieved / peak, "traffic": traffic, "peak_kind": peak_kind,
+                         "bytes_per_cell": bpc, "kernel": "fused_kernel (one launch per step)"},
+            "clocks": clk.summary()}
+    if not a.no_extras:
+        line["e2e"] = time_e2e(sim, p, 5, stream)
+        if rank == 0:
+            line["error_vs_fp64"] = error_vs_fp64(a.workload, a.precision, local) if a.precision != "fp64" else None
+            variants = {}
+            for prec in ("fp64", "fp16"):
+                if prec == a.precision:
+                    continue
+                s2, _ = make_sim(a.workload, prec, local)
+                s2.set_stream(stream.cuda_stream)
+                n2 = max(200, a.steps // 5)
+                ms2, _ = time_device(s2, n2, 10, stream)
+                variants[prec] = {"value": V * n2 / (ms2 * 1e3), "unit": "MLUPS", "steps": n2,
+                                  "frac": BYTES_PER_CELL[prec] * V / (ms2 / n2 * 1e-3) / 1e9 / peak}
+                s2.close()
+            line["variants"] = variants
+            try:
+                line["cpu_baseline"] = {k: v for k, v in reference_cpu(a.workload, 5 if V > 1e6 else 50, 1).items()
+                                        if k != "ms_step"}
+            except Exception as e:  # the baseline is reported, never required
+                line["cpu_baseline"] = {"value": None, "unit": "MLUPS", "error": str(e)[:200]}
+    sim.close()
+    if rank == 0:
+        print(json.dumps(line), flush=True)
+    if world > 1:
+        dist.barrier()
+        dist.destroy_process_group()
+
+
+if __name__ == "__main__":
+    main()

@@ -1,0 +1,165 @@
+/*
+ * lbman3d.h -- C ABI of the B200 (sm_100a) implementation of lbman3d's
+ * per-timestep hot path: the D3Q15 lattice-Boltzmann collide/stream, the
+ * Beris-Edwards Q-tensor step with the active/passive body force, every wall
+ * rule of the reference, and the diagnostic reductions.
+ *
+ * Plain C: pointers, sizes and int status codes, no C++ or torch types.
+ * Host buffers are always float64 in the reference's host layout
+ * (x fastest, cell = (z*ny + y)*nx + x); vector fields are 3 consecutive
+ * blocks of V = nx*ny*nz values, Q is 5 blocks (xx, xy, xz, yy, yz) and
+ * populations are 15 blocks, direction-major (f[i*V + cell], the
+ * reference's device layout, src/local_grid.h:64).  Device memory is owned by
+ * the library; host memory by the caller.
+ *
+ * Every entry point returns LBMAN_OK (0) or an error code; lbman_last_error()
+ * gives a message for the calling thread.  A thin C++ layer
+ * (include/lbman3d_dropin.hpp) maps the reference's DeviceFields /
+ * DeviceSolver<BC> / LbmSolver<BC> / QTensorSolver<BC> onto these calls and
+ * throws std::runtime_error on a non-zero status, the reference's error
+ * convention (src/cuda/cuda_utils.h:5-10).
+ */
+#ifndef LBMAN3D_H_
+#define LBMAN3D_H_
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define LBMAN_ABI_VERSION 1
+
+/* Status codes. */
+#define LBMAN_OK 0
+#define LBMAN_ERR_ARG 1         /* invalid argument or configuration            */
+#define LBMAN_ERR_CUDA 2        /* a CUDA call failed                            */
+#define LBMAN_ERR_DIVERGED 3    /* NaN in the global mass or momentum            */
+#define LBMAN_ERR_TIMEOUT 4     /* a bounded device wait gave up                 */
+#define LBMAN_ERR_STATE 5       /* call out of order (e.g. step before upload)   */
+#define LBMAN_ERR_UNSUPPORTED 6 /* configuration this build does not implement   */
+#define LBMAN_ERR_NOMEM 7       /* device allocation failed                      */
+
+/* Q-tensor wall tags (src/boundary.h:31-42). */
+#define LBMAN_Q_PERIODIC 0
+#define LBMAN_Q_NEUMANN 1
+#define LBMAN_Q_ANCHORING 2
+/* Velocity wall tags (src/boundary.h:31-50). */
+#define LBMAN_U_PERIODIC 0
+#define LBMAN_U_NOSLIP 1
+#define LBMAN_U_MOVING 2
+#define LBMAN_U_SPECULAR 3
+/* Advection scheme (src/qtensor_types.h:19, kQAdvection). */
+#define LBMAN_CENTRED 0
+#define LBMAN_UPWIND 1
+/* Storage / compute precision. */
+#define LBMAN_FP64 0 /* FP64 compute and storage, the reference's arithmetic   */
+#define LBMAN_FP32 1 /* FP32 compute, populations stored as f_i - w_i*rho0    */
+#define LBMAN_FP16 2 /* FP32 compute, populations stored as FP16 deviations   */
+/* Kernel organisation. */
+#define LBMAN_KERNELS_AUTO 0
+#define LBMAN_KERNELS_SPLIT 1 /* Q+force kernel, then LBM kernel               */
+#define LBMAN_KERNELS_FUSED 2 /* one kernel per time step                      */
+
+/* One face of the box: WallSpec<QBC, UBC> (src/boundary.h:72-76). */
+typedef struct lbman_face {
+    int qbc;                  /* LBMAN_Q_*                                  */
+    double s, theta, phi;     /* Anchoring<S, theta, phi> (radians)          */
+    int ubc;                  /* LBMAN_U_*                                  */
+    double uw[3];             /* MovingWall<Ux, Uy, Uz>                      */
+} lbman_face;
+
+/* Runtime form of params.h + sim_config.h + the BC type (SimBC). */
+typedef struct lbman_config {
+    int nx, ny, nz;
+    double DT, kDensity, TAUF, L, A, B, C, LAMBDA, GAMMA, ALPHA, MU;
+    int advection;            /* LBMAN_CENTRED / LBMAN_UPWIND                */
+    lbman_face face[6];       /* XLo, XHi, YLo, YHi, ZLo, ZHi                */
+    int precision;            /* LBMAN_FP64 / LBMAN_FP32 / LBMAN_FP16        */
+    int kernels;              /* LBMAN_KERNELS_*                             */
+    int device;               /* CUDA device ordinal                         */
+    int tile_x, tile_y, zchunk, threads; /* 0 = library default           */
+} lbman_config;
+
+/* Global diagnostics (src/sim_io.cc:78-166, src/analysis_fields.h:39-72). */
+typedef struct lbman_diag {
+    double mass, px, py, pz;  /* sum rho, sum rho*u                          */
+    double kinetic_energy;    /* sum rho*|u|^2/2                             */
+    double rel_change_num;    /* sum |u - u_prev|^2 since the previous call  */
+    double rel_change_den;    /* sum |u|^2                                   */
+    double umax2;             /* max |u|^2                                   */
+    double free_energy;       /* TotalNematicFreeEnergy (LBMAN_DIAG_ENERGY)  */
+    int64_t defect_faces;     /* plaquettes with a director sign flip
+                                 (LBMAN_DIAG_DEFECTS), -1 if not computed    */
+    int nan_detected;         /* NaN in mass or momentum                     */
+} lbman_diag;
+
+#define LBMAN_DIAG_FLOW 1     /* mass, momentum, kinetic energy, max |u|       */
+#define LBMAN_DIAG_ENERGY 2   /* nematic free energy                          */
+#define LBMAN_DIAG_DEFECTS 4  /* director sign-flip plaquette count           */
+#define LBMAN_DIAG_ALL 7
+
+typedef struct lbman_solver lbman_solver;
+
+/* params.h defaults (src/params.h:14-112), SimBC = SlitNoSlipConfig, FP64. */
+int lbman_config_init(lbman_config* cfg);
+const char* lbman_status_string(int status);
+const char* lbman_last_error(void);
+int lbman_abi_version(void);
+
+/* Device description, InitializeComputeBackend (src/device_fields.h:21). */
+int lbman_device_info(int device, char* buf, size_t len);
+
+/* DeviceFields(LocalGrid) + DeviceSolver<BC>::Initialize
+ * (src/device_fields.h:174, src/device_solver.h:15).  Rejects an axis whose
+ * velocity tag is periodic on one face only.                                */
+int lbman_create(const lbman_config* cfg, lbman_solver** out);
+int lbman_destroy(lbman_solver* s);
+/* Issue all work on this cudaStream_t (default: a stream owned by s).        */
+int lbman_set_stream(lbman_solver* s, void* cuda_stream);
+int lbman_synchronize(lbman_solver* s);
+
+/* DeviceFields::Initialize(FluidFields&, const QTensorFields&)
+ * (src/device_fields.h:179).  rho[V], u3[3V], q5[5V] required; f15 (15V,
+ * direction-major) NULL means f = f_eq(rho, u) as LbmSolver::Initialize
+ * (src/lbm_solver.tpp:35-62); force3 NULL means zero body force.            */
+int lbman_upload(lbman_solver* s, const double* rho, const double* u3, const double* q5,
+                 const double* f15, const double* force3);
+/* Seeded initial state generated on the device (no host transfer): rho =
+ * kDensity, u = 0, zero body force, Q = S0 (n n^T - I/3) with n uniform on
+ * the sphere per cell plus N(0, sigma^2) on each stored Q component
+ * (counter-based splitmix64 of seed and cell index), f = f_eq.  This is the
+ * initial condition of every benchmark workload; it replaces the
+ * reference's unseeded QTensorSolver::Initialize
+ * (src/qtensor_solver.tpp:14-48) the way its tests override Initialize.    */
+int lbman_init_seeded(lbman_solver* s, uint64_t seed, double S0, double sigma);
+
+/* DeviceFields::CopyToHost (src/device_fields.h:181); any pointer may be NULL.
+ * f15 receives the pre-collision populations, as the reference stores them. */
+int lbman_download(lbman_solver* s, double* rho, double* u3, double* q5, double* f15,
+                   double* force3);
+
+/* ActiveNematicSim::Step (src/active_nematic.h:104-108), n times.            */
+int lbman_step(lbman_solver* s, int nsteps);
+/* DeviceSolver<BC>::QTensorStep: Q update + full body force
+ * (src/cuda/device_solver.cu:35-98).                                         */
+int lbman_qtensor_step(lbman_solver* s);
+/* DeviceSolver<BC>::LBMStep: collide + stream + walls with the current body
+ * force (src/cuda/device_solver.cu:101-121).                                 */
+int lbman_lbm_step(lbman_solver* s);
+
+/* SimIO::Log reductions + TotalNematicFreeEnergy + defect plaquettes, FP64
+ * accumulation on the device.  Returns LBMAN_ERR_DIVERGED (after filling out)
+ * when the mass or momentum is NaN, as SimIO::Log returns false.            */
+int lbman_reduce(lbman_solver* s, int flags, lbman_diag* out);
+
+/* Steps completed since the last upload. */
+int lbman_steps_done(lbman_solver* s, int64_t* steps);
+/* Kernel launches issued by this solver since creation (instrumentation).  */
+int lbman_launch_count(lbman_solver* s, int64_t* launches);
+
+#ifdef __cplusplus
+}
+#endif
+#endif

@@ -1,0 +1,114 @@
+"""ctypes binding of include/lbman3d.h (liblbman3d_b200.so, built in tree).
+
+The shared library is the product: there is no Python or CPU fallback.  If
+it is missing, every entry point raises ImportError with the build command.
+"""
+from __future__ import annotations
+
+import ctypes as C
+import os
+
+PKG = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(PKG, "liblbman3d_b200.so")
+
+OK, ERR_ARG, ERR_CUDA, ERR_DIVERGED, ERR_TIMEOUT, ERR_STATE, ERR_UNSUPPORTED, ERR_NOMEM = range(8)
+Q_PERIODIC, Q_NEUMANN, Q_ANCHORING = 0, 1, 2
+U_PERIODIC, U_NOSLIP, U_MOVING, U_SPECULAR = 0, 1, 2, 3
+CENTRED, UPWIND = 0, 1
+FP64, FP32, FP16 = 0, 1, 2
+KERNELS_AUTO, KERNELS_SPLIT, KERNELS_FUSED = 0, 1, 2
+DIAG_FLOW, DIAG_ENERGY, DIAG_DEFECTS, DIAG_ALL = 1, 2, 4, 7
+
+
+class lbman_face(C.Structure):
+    _fields_ = [("qbc", C.c_int), ("s", C.c_double), ("theta", C.c_double), ("phi", C.c_double),
+                ("ubc", C.c_int), ("uw", C.c_double * 3)]
+
+
+class lbman_config(C.Structure):
+    _fields_ = [("nx", C.c_int), ("ny", C.c_int), ("nz", C.c_int),
+                ("DT", C.c_double), ("kDensity", C.c_double), ("TAUF", C.c_double),
+                ("L", C.c_double), ("A", C.c_double), ("B", C.c_double), ("C", C.c_double),
+                ("LAMBDA", C.c_double), ("GAMMA", C.c_double), ("ALPHA", C.c_double),
+                ("MU", C.c_double), ("advection", C.c_int), ("face", lbman_face * 6),
+                ("precision", C.c_int), ("kernels", C.c_int), ("device", C.c_int),
+                ("tile_x", C.c_int), ("tile_y", C.c_int), ("zchunk", C.c_int), ("threads", C.c_int)]
+
+
+class lbman_diag(C.Structure):
+    _fields_ = [("mass", C.c_double), ("px", C.c_double), ("py", C.c_double), ("pz", C.c_double),
+                ("kinetic_energy", C.c_double), ("rel_change_num", C.c_double),
+                ("rel_change_den", C.c_double), ("umax2", C.c_double), ("free_energy", C.c_double),
+                ("defect_faces", C.c_int64), ("nan_detected", C.c_int)]
+
+
+class LbmanError(RuntimeError):
+    """A non-zero status from the C ABI (the reference throws std::runtime_error)."""
+
+    def __init__(self, status: int, message: str):
+        super().__init__(f"lbman status {status}: {message}")
+        self.status = status
+
+
+class DivergedError(LbmanError):
+    pass
+
+
+_lib = None
+
+# (name, restype, argtypes) for every entry point declared in include/lbman3d.h
+_DP = C.POINTER(C.c_double)
+PROTOTYPES = [
+    ("lbman_config_init", C.c_int, [C.POINTER(lbman_config)]),
+    ("lbman_status_string", C.c_char_p, [C.c_int]),
+    ("lbman_last_error", C.c_char_p, []),
+    ("lbman_abi_version", C.c_int, []),
+    ("lbman_device_info", C.c_int, [C.c_int, C.c_char_p, C.c_size_t]),
+    ("lbman_create", C.c_int, [C.POINTER(lbman_config), C.POINTER(C.c_void_p)]),
+    ("lbman_destroy", C.c_int, [C.c_void_p]),
+    ("lbman_set_stream", C.c_int, [C.c_void_p, C.c_void_p]),
+    ("lbman_synchronize", C.c_int, [C.c_void_p]),
+    ("lbman_upload", C.c_int, [C.c_void_p, _DP, _DP, _DP, _DP, _DP]),
+    ("lbman_init_seeded", C.c_int, [C.c_void_p, C.c_uint64, C.c_double, C.c_double]),
+    ("lbman_download", C.c_int, [C.c_void_p, _DP, _DP, _DP, _DP, _DP]),
+    ("lbman_step", C.c_int, [C.c_void_p, C.c_int]),
+    ("lbman_qtensor_step", C.c_int, [C.c_void_p]),
+    ("lbman_lbm_step", C.c_int, [C.c_void_p]),
+    ("lbman_reduce", C.c_int, [C.c_void_p, C.c_int, C.POINTER(lbman_diag)]),
+    ("lbman_steps_done", C.c_int, [C.c_void_p, C.POINTER(C.c_int64)]),
+    ("lbman_launch_count", C.c_int, [C.c_void_p, C.POINTER(C.c_int64)]),
+]
+
+
+def lib():
+    """Load liblbman3d_b200.so (once).  Raises ImportError if it is not built."""
+    global _lib
+    if _lib is None:
+        if not os.path.exists(LIB_PATH):
+            raise ImportError(f"{LIB_PATH} is missing; build it with `python -m lbman3d_b200.build` "
+                              "(nvcc, sm_100a). There is no CPU fallback.")
+        L = C.CDLL(LIB_PATH)
+        for name, res, args in PROTOTYPES:
+            fn = getattr(L, name)
+            fn.restype = res
+            fn.argtypes = args
+        _lib = L
+    return _lib
+
+
+def check(status: int):
+    if status != OK:
+        msg = lib().lbman_last_error().decode(errors="replace")
+        if status == ERR_DIVERGED:
+            raise DivergedError(status, msg)
+        raise LbmanError(status, msg)
+    return status
+
+
+def dptr(a):
+    """float64 C-contiguous numpy array -> double*, None -> NULL."""
+    if a is None:
+        return None
+    if a.dtype.name != "float64" or not a.flags.c_contiguous:
+        raise TypeError("host buffers must be C-contiguous float64 arrays")
+    return a.ctypes.data_as(_DP)

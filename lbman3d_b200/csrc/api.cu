@@ -1,0 +1,552 @@
+// api.cu -- the C ABI of include/lbman3d.h: device memory, launch sequencing
+// and error reporting.  Host code only; the kernels live in kernels_*.cu.
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <cmath>
+#include <cstdarg>
+#include <cstdio>
+#include <cstring>
+#include <string>
+
+#include "../../include/lbman3d.h"
+#include "launch.h"
+
+using namespace lbman;
+
+namespace {
+
+thread_local std::string g_err;
+
+int fail(int code, const char* fmt, ...) {
+    char buf[512];
+    va_list ap;
+    va_start(ap, fmt);
+    vsnprintf(buf, sizeof(buf), fmt, ap);
+    va_end(ap);
+    g_err = buf;
+    return code;
+}
+
+#define LB_CUDA(call)                                                                             \
+    do {                                                                                          \
+        cudaError_t e_ = (call);                                                                  \
+        if (e_ != cudaSuccess)                                                                    \
+            return fail(e_ == cudaErrorMemoryAllocation ? LBMAN_ERR_NOMEM : LBMAN_ERR_CUDA,       \
+                        "%s:%d %s: %s", __FILE__, __LINE__, #call, cudaGetErrorString(e_));       \
+    } while (0)
+
+#define LB_TRY(expr)                  \
+    do {                              \
+        int s_ = (expr);              \
+        if (s_ != LBMAN_OK) return s_; \
+    } while (0)
+
+struct Ops {
+    decltype(&launch_qforce_f64) qforce;
+    decltype(&launch_fused_f64) fused;
+    decltype(&launch_lbm_f64) lbm;
+    decltype(&launch_stream_only_f64) stream_only;
+    decltype(&launch_feq_init_f64) feq_init;
+    decltype(&launch_pop_in_f64) pop_in;
+    decltype(&launch_pop_out_f64) pop_out;
+    decltype(&launch_real_in_f64) real_in;
+    decltype(&launch_real_out_f64) real_out;
+    decltype(&launch_flow_reduce_f64) flow_reduce;
+    decltype(&launch_energy_reduce_f64) energy_reduce;
+    decltype(&launch_director_f64) director;
+    decltype(&launch_defect_count_f64) defect_count;
+    decltype(&launch_seeded_init_f64) seeded_init;
+    decltype(&qforce_smem_f64) qforce_smem;
+    decltype(&prepare_f64) prepare;
+};
+
+#define LBMAN_OPS(SUF)                                                                                 \
+    Ops {                                                                                              \
+        launch_qforce_##SUF, launch_fused_##SUF, launch_lbm_##SUF, launch_stream_only_##SUF,           \
+            launch_feq_init_##SUF, launch_pop_in_##SUF, launch_pop_out_##SUF, launch_real_in_##SUF,    \
+            launch_real_out_##SUF, launch_flow_reduce_##SUF, launch_energy_reduce_##SUF,               \
+            launch_director_##SUF, launch_defect_count_##SUF, launch_seeded_init_##SUF,               \
+            qforce_smem_##SUF, prepare_##SUF                                                           \
+    }
+
+const Ops kOps[3] = {LBMAN_OPS(f64), LBMAN_OPS(f32), LBMAN_OPS(f16)};
+
+// AnchoredQ (src/boundary_handler.h:232-251), evaluated on the host.
+void anchored_q(const lbman_face& f, double out[5]) {
+    if (f.qbc != LBMAN_Q_ANCHORING) {
+        for (int k = 0; k < 5; ++k) out[k] = 0.0;
+        return;
+    }
+    const double sin_sq_phi = 0.5 * (1.0 - std::cos(2.0 * f.phi));
+    const double cos_sq_phi = 1.0 - sin_sq_phi;
+    const double sin_phi_cos_phi = 0.5 * std::sin(2.0 * f.phi);
+    const double sin_sq_th = 0.5 * (1.0 - std::cos(2.0 * f.theta));
+    const double sin_th_cos_th = 0.5 * std::sin(2.0 * f.theta);
+    const double S = f.s;
+    out[0] = S * (cos_sq_phi * sin_sq_th - 1.0 / 3.0);
+    out[1] = S * (sin_phi_cos_phi * sin_sq_th);
+    out[2] = S * (std::cos(f.phi) * sin_th_cos_th);
+    out[3] = S * (sin_sq_phi * sin_sq_th - 1.0 / 3.0);
+    out[4] = S * (std::sin(f.phi) * sin_th_cos_th);
+}
+
+}  // namespace
+
+struct lbman_solver {
+    lbman_config cfg;
+    SimParams P;
+    LaunchShape shape;
+    int prec = LBMAN_FP64;
+    int kernels = LBMAN_KERNELS_FUSED;
+    int device = 0;
+    size_t rbytes = 8, sbytes = 8;
+    void* f[2] = {nullptr, nullptr};
+    void* q[2] = {nullptr, nullptr};
+    void* u[2] = {nullptr, nullptr};
+    void* rho = nullptr;
+    void* F = nullptr;
+    double* staging = nullptr;
+    double* partials = nullptr;
+    int red_G = 0;
+    double* red_dev = nullptr;
+    double* red_host = nullptr;
+    void* upast = nullptr;
+    void* dirbuf = nullptr;
+    int fcur = 0, qcur = 0, ucur = 0;
+    bool uploaded = false, f_post = false;
+    cudaStream_t stream = nullptr;
+    bool own_stream = false;
+    int64_t steps = 0, launches = 0;
+    int num_sms = 148;
+    const Ops& ops() const { return kOps[prec]; }
+};
+
+namespace {
+
+int set_device(lbman_solver* s) {
+    LB_CUDA(cudaSetDevice(s->device));
+    return LBMAN_OK;
+}
+
+int check_launch(lbman_solver* s, cudaError_t e, const char* what) {
+    ++s->launches;
+    if (e != cudaSuccess) return fail(LBMAN_ERR_CUDA, "%s launch failed: %s", what, cudaGetErrorString(e));
+    return LBMAN_OK;
+}
+
+// Default z-marching shape: tile 30 x 6 (B region 32 x 8 = 256 points, one
+// per thread), z chunks sized for several waves of blocks.
+LaunchShape default_shape(const lbman_config& c, int num_sms) {
+    LaunchShape L;
+    L.tile.tcx = c.tile_x > 0 ? c.tile_x : 30;
+    L.tile.tcy = c.tile_y > 0 ? c.tile_y : 6;
+    const int bpts = (L.tile.tcx + 2) * (L.tile.tcy + 2);
+    L.qthreads = c.threads > 0 ? c.threads : std::min(512, ((bpts + 31) / 32) * 32);
+    if (c.zchunk > 0) {
+        L.tile.zc = c.zchunk;
+    } else {
+        const long cols = (long)((c.nx + L.tile.tcx - 1) / L.tile.tcx) * ((c.ny + L.tile.tcy - 1) / L.tile.tcy);
+        const long target = (long)num_sms * 8;
+        long nchunks = (target + cols - 1) / cols;
+        nchunks = std::max(1L, std::min(nchunks, (long)std::max(1, c.nz / 8)));
+        L.tile.zc = (int)((c.nz + nchunks - 1) / nchunks);
+    }
+    return L;
+}
+
+int validate(const lbman_config& c) {
+    if (c.nx < 1 || c.ny < 1 || c.nz < 1) return fail(LBMAN_ERR_ARG, "grid must be at least 1x1x1");
+    const double V = (double)c.nx * c.ny * c.nz;
+    if (V >= 2147483648.0) return fail(LBMAN_ERR_UNSUPPORTED, "grids of 2^31 cells or more are not supported");
+    if (c.precision < LBMAN_FP64 || c.precision > LBMAN_FP16) return fail(LBMAN_ERR_ARG, "bad precision");
+    if (c.advection != LBMAN_CENTRED && c.advection != LBMAN_UPWIND) return fail(LBMAN_ERR_ARG, "bad advection");
+    if (c.kernels < LBMAN_KERNELS_AUTO || c.kernels > LBMAN_KERNELS_FUSED) return fail(LBMAN_ERR_ARG, "bad kernels");
+    if (!(c.TAUF > 0.0) || !(c.DT > 0.0) || !(c.kDensity > 0.0)) return fail(LBMAN_ERR_ARG, "TAUF, DT, kDensity must be > 0");
+    for (int k = 0; k < 6; ++k) {
+        const lbman_face& f = c.face[k];
+        if (f.qbc < LBMAN_Q_PERIODIC || f.qbc > LBMAN_Q_ANCHORING) return fail(LBMAN_ERR_ARG, "face %d: bad Q tag", k);
+        if (f.ubc < LBMAN_U_PERIODIC || f.ubc > LBMAN_U_SPECULAR) return fail(LBMAN_ERR_ARG, "face %d: bad velocity tag", k);
+    }
+    for (int ax = 0; ax < 3; ++ax) {
+        const bool lo = c.face[2 * ax].ubc == LBMAN_U_PERIODIC, hi = c.face[2 * ax + 1].ubc == LBMAN_U_PERIODIC;
+        if (lo != hi)
+            return fail(LBMAN_ERR_ARG,
+                        "axis %c: the velocity tag is periodic on one face only; streaming across such an axis "
+                        "has two writers per population in the reference and is not supported",
+                        "xyz"[ax]);
+    }
+    if (c.tile_x < 0 || c.tile_y < 0 || c.zchunk < 0 || c.threads < 0) return fail(LBMAN_ERR_ARG, "bad launch shape");
+    return LBMAN_OK;
+}
+
+int stage_in_real(lbman_solver* s, const double* host, void* dst, int64_t n) {
+    if (s->prec == LBMAN_FP64) {
+        LB_CUDA(cudaMemcpyAsync(dst, host, n * sizeof(double), cudaMemcpyHostToDevice, s->stream));
+        return LBMAN_OK;
+    }
+    LB_CUDA(cudaMemcpyAsync(s->staging, host, n * sizeof(double), cudaMemcpyHostToDevice, s->stream));
+    return check_launch(s, s->ops().real_in(s->staging, dst, n, s->stream), "real_in");
+}
+
+int stage_out_real(lbman_solver* s, const void* src, double* host, int64_t n) {
+    if (s->prec == LBMAN_FP64) {
+        LB_CUDA(cudaMemcpyAsync(host, src, n * sizeof(double), cudaMemcpyDeviceToHost, s->stream));
+        return LBMAN_OK;
+    }
+    LB_TRY(check_launch(s, s->ops().real_out(src, s->staging, n, s->stream), "real_out"));
+    LB_CUDA(cudaMemcpyAsync(host, s->staging, n * sizeof(double), cudaMemcpyDeviceToHost, s->stream));
+    return LBMAN_OK;
+}
+
+void* vptr(void* base, int64_t off_elems, size_t esize) { return (char*)base + off_elems * (int64_t)esize; }
+
+}  // namespace
+
+extern "C" {
+
+int lbman_abi_version(void) { return LBMAN_ABI_VERSION; }
+
+const char* lbman_last_error(void) { return g_err.c_str(); }
+
+const char* lbman_status_string(int status) {
+    switch (status) {
+        case LBMAN_OK: return "ok";
+        case LBMAN_ERR_ARG: return "invalid argument";
+        case LBMAN_ERR_CUDA: return "CUDA error";
+        case LBMAN_ERR_DIVERGED: return "simulation diverged (NaN in mass or momentum)";
+        case LBMAN_ERR_TIMEOUT: return "bounded device wait timed out";
+        case LBMAN_ERR_STATE: return "call out of order";
+        case LBMAN_ERR_UNSUPPORTED: return "unsupported configuration";
+        case LBMAN_ERR_NOMEM: return "device allocation failed";
+        default: return "unknown status";
+    }
+}
+
+int lbman_config_init(lbman_config* c) {
+    if (!c) return fail(LBMAN_ERR_ARG, "null config");
+    std::memset(c, 0, sizeof(*c));
+    // src/params.h:14-112
+    c->nx = 20; c->ny = 100; c->nz = 100;
+    c->DT = 1.0; c->kDensity = 1.0; c->TAUF = 2.5 * 1.0;
+    c->L = 0.06; c->A = 0.0; c->B = -0.3; c->C = 0.3;
+    c->LAMBDA = 0.3; c->GAMMA = 0.34; c->ALPHA = 0.023; c->MU = 0.0;
+    c->advection = LBMAN_CENTRED;
+    // SimBC = SlitNoSlipConfig (src/sim_config.h:37-48)
+    for (int k = 0; k < 6; ++k) { c->face[k].qbc = LBMAN_Q_PERIODIC; c->face[k].ubc = LBMAN_U_PERIODIC; }
+    c->face[0].qbc = c->face[1].qbc = LBMAN_Q_NEUMANN;
+    c->face[0].ubc = c->face[1].ubc = LBMAN_U_NOSLIP;
+    c->precision = LBMAN_FP64;
+    c->kernels = LBMAN_KERNELS_AUTO;
+    c->device = 0;
+    return LBMAN_OK;
+}
+
+int lbman_device_info(int device, char* buf, size_t len) {
+    if (!buf || len == 0) return fail(LBMAN_ERR_ARG, "null buffer");
+    cudaDeviceProp p;
+    LB_CUDA(cudaGetDeviceProperties(&p, device));
+    size_t fr = 0, tot = 0;
+    LB_CUDA(cudaSetDevice(device));
+    LB_CUDA(cudaMemGetInfo(&fr, &tot));
+    snprintf(buf, len,
+             "GPU\n       using device: %d\n               name: %s\n    multiprocessors: %d\n"
+             " compute capability: %d.%d\n      global memory: %.1f MiB\n        free memory: %.1f MiB\n",
+             device, p.name, p.multiProcessorCount, p.major, p.minor, tot / 1048576.0, fr / 1048576.0);
+    return LBMAN_OK;
+}
+
+int lbman_create(const lbman_config* cfg, lbman_solver** out) {
+    if (!cfg || !out) return fail(LBMAN_ERR_ARG, "null argument");
+    *out = nullptr;
+    LB_TRY(validate(*cfg));
+    lbman_solver* s = new lbman_solver();
+    s->cfg = *cfg;
+    s->device = cfg->device;
+    s->prec = cfg->precision;
+    s->kernels = cfg->kernels == LBMAN_KERNELS_AUTO ? LBMAN_KERNELS_FUSED : cfg->kernels;
+    s->rbytes = s->prec == LBMAN_FP64 ? 8 : 4;
+    s->sbytes = s->prec == LBMAN_FP64 ? 8 : (s->prec == LBMAN_FP32 ? 4 : 2);
+    auto bail = [&](int code) {
+        lbman_destroy(s);
+        return code;
+    };
+    if (int st = set_device(s)) return bail(st);
+    cudaDeviceProp prop;
+    if (cudaGetDeviceProperties(&prop, s->device) != cudaSuccess)
+        return bail(fail(LBMAN_ERR_CUDA, "cudaGetDeviceProperties failed"));
+    if (prop.major < 10) return bail(fail(LBMAN_ERR_UNSUPPORTED, "this build targets sm_100a (B200); device is sm_%d%d", prop.major, prop.minor));
+    s->num_sms = prop.multiProcessorCount;
+
+    SimParams& P = s->P;
+    std::memset(&P, 0, sizeof(P));
+    P.nx = cfg->nx; P.ny = cfg->ny; P.nz = cfg->nz;
+    P.nxy = (int64_t)cfg->nx * cfg->ny;
+    P.V = P.nxy * cfg->nz;
+    P.DT = cfg->DT; P.kDensity = cfg->kDensity; P.L = cfg->L; P.A = cfg->A; P.B = cfg->B; P.C = cfg->C;
+    P.LAMBDA = cfg->LAMBDA; P.GAMMA = cfg->GAMMA; P.ALPHA = cfg->ALPHA; P.MU = cfg->MU;
+    // src/params.h:52-54
+    P.omega = 1.0 - cfg->DT / cfg->TAUF;
+    P.omega_prime = cfg->DT / cfg->TAUF;
+    P.omega_forcing = 1.0 - cfg->DT / 2.0 / cfg->TAUF;
+    P.upwind = cfg->advection == LBMAN_UPWIND;
+    P.moving_any = 0;
+    for (int k = 0; k < 6; ++k) {
+        P.face[k].qbc = cfg->face[k].qbc;
+        P.face[k].ubc = cfg->face[k].ubc;
+        anchored_q(cfg->face[k], P.face[k].anchor);
+        for (int j = 0; j < 3; ++j) P.face[k].uw[j] = cfg->face[k].ubc == LBMAN_U_MOVING ? cfg->face[k].uw[j] : 0.0;
+        P.qper[k] = cfg->face[k].qbc == LBMAN_Q_PERIODIC;
+        P.uper[k] = cfg->face[k].ubc == LBMAN_U_PERIODIC;
+        if (cfg->face[k].ubc == LBMAN_U_MOVING) P.moving_any = 1;
+    }
+
+    s->shape = default_shape(*cfg, s->num_sms);
+    const size_t smem = s->ops().qforce_smem(s->shape.tile);
+    if (smem > (size_t)prop.sharedMemPerBlockOptin)
+        return bail(fail(LBMAN_ERR_ARG, "tile %dx%d needs %zu B of shared memory (max %zu)", s->shape.tile.tcx,
+                         s->shape.tile.tcy, smem, (size_t)prop.sharedMemPerBlockOptin));
+    if (s->shape.qthreads % 32 || s->shape.qthreads > 512 || s->shape.qthreads < 32)
+        return bail(fail(LBMAN_ERR_ARG, "threads must be a multiple of 32 in [32, 512]"));
+    if (cudaError_t e = s->ops().prepare(prop.sharedMemPerBlockOptin))
+        return bail(fail(LBMAN_ERR_CUDA, "cudaFuncSetAttribute: %s", cudaGetErrorString(e)));
+
+    const int64_t V = P.V;
+    auto alloc = [&](void** p, size_t bytes) -> int {
+        cudaError_t e = cudaMalloc(p, bytes);
+        if (e != cudaSuccess) return fail(LBMAN_ERR_NOMEM, "cudaMalloc(%zu) failed: %s", bytes, cudaGetErrorString(e));
+        return LBMAN_OK;
+    };
+    for (int b = 0; b < 2; ++b) {
+        if (int st = alloc(&s->f[b], 15 * V * s->sbytes)) return bail(st);
+        if (int st = alloc(&s->q[b], 5 * V * s->rbytes)) return bail(st);
+        if (int st = alloc(&s->u[b], 3 * V * s->rbytes)) return bail(st);
+    }
+    if (int st = alloc(&s->rho, V * s->rbytes)) return bail(st);
+    if (int st = alloc(&s->F, 3 * V * s->rbytes)) return bail(st);
+    if (s->prec != LBMAN_FP64)
+        if (int st = alloc((void**)&s->staging, V * sizeof(double))) return bail(st);
+    s->red_G = (int)std::min<int64_t>((V + 255) / 256, (int64_t)s->num_sms * 8);
+    if (int st = alloc((void**)&s->partials, (size_t)s->red_G * 8 * sizeof(double))) return bail(st);
+    if (int st = alloc((void**)&s->red_dev, 16 * sizeof(double))) return bail(st);
+    if (cudaMallocHost((void**)&s->red_host, 16 * sizeof(double)) != cudaSuccess)
+        return bail(fail(LBMAN_ERR_NOMEM, "cudaMallocHost failed"));
+    if (cudaStreamCreateWithFlags(&s->stream, cudaStreamNonBlocking) != cudaSuccess)
+        return bail(fail(LBMAN_ERR_CUDA, "cudaStreamCreate failed"));
+    s->own_stream = true;
+    *out = s;
+    return LBMAN_OK;
+}
+
+int lbman_destroy(lbman_solver* s) {
+    if (!s) return LBMAN_OK;
+    cudaSetDevice(s->device);
+    if (s->stream) cudaStreamSynchronize(s->stream);
+    for (int b = 0; b < 2; ++b) { cudaFree(s->f[b]); cudaFree(s->q[b]); cudaFree(s->u[b]); }
+    cudaFree(s->rho); cudaFree(s->F); cudaFree(s->staging); cudaFree(s->partials); cudaFree(s->red_dev);
+    cudaFree(s->upast); cudaFree(s->dirbuf);
+    if (s->red_host) cudaFreeHost(s->red_host);
+    if (s->own_stream && s->stream) cudaStreamDestroy(s->stream);
+    delete s;
+    return LBMAN_OK;
+}
+
+int lbman_set_stream(lbman_solver* s, void* stream) {
+    if (!s) return fail(LBMAN_ERR_ARG, "null solver");
+    LB_TRY(set_device(s));
+    LB_CUDA(cudaStreamSynchronize(s->stream));
+    if (s->own_stream) cudaStreamDestroy(s->stream);
+    s->stream = (cudaStream_t)stream;
+    s->own_stream = false;
+    return LBMAN_OK;
+}
+
+int lbman_synchronize(lbman_solver* s) {
+    if (!s) return fail(LBMAN_ERR_ARG, "null solver");
+    LB_TRY(set_device(s));
+    LB_CUDA(cudaStreamSynchronize(s->stream));
+    return LBMAN_OK;
+}
+
+int lbman_upload(lbman_solver* s, const double* rho, const double* u3, const double* q5, const double* f15,
+                 const double* force3) {
+    if (!s || !rho || !u3 || !q5) return fail(LBMAN_ERR_ARG, "rho, u and q are required");
+    LB_TRY(set_device(s));
+    const int64_t V = s->P.V;
+    LB_TRY(stage_in_real(s, rho, s->rho, V));
+    for (int k = 0; k < 3; ++k) LB_TRY(stage_in_real(s, u3 + k * V, vptr(s->u[s->ucur], k * V, s->rbytes), V));
+    for (int k = 0; k < 5; ++k) LB_TRY(stage_in_real(s, q5 + k * V, vptr(s->q[s->qcur], k * V, s->rbytes), V));
+    if (force3) {
+        for (int k = 0; k < 3; ++k) LB_TRY(stage_in_real(s, force3 + k * V, vptr(s->F, k * V, s->rbytes), V));
+    } else {
+        LB_CUDA(cudaMemsetAsync(s->F, 0, 3 * V * s->rbytes, s->stream));
+    }
+    if (f15) {
+        for (int j = 0; j < 15; ++j) {
+            if (s->prec == LBMAN_FP64) {
+                LB_CUDA(cudaMemcpyAsync(vptr(s->f[s->fcur], j * V, 8), f15 + j * V, V * 8, cudaMemcpyHostToDevice, s->stream));
+            } else {
+                LB_CUDA(cudaMemcpyAsync(s->staging, f15 + j * V, V * 8, cudaMemcpyHostToDevice, s->stream));
+                LB_TRY(check_launch(s, s->ops().pop_in(s->P, s->staging, s->f[s->fcur], j, s->stream), "pop_in"));
+            }
+        }
+    } else {
+        LB_TRY(check_launch(s, s->ops().feq_init(s->P, s->rho, s->u[s->ucur], s->f[s->fcur], s->stream), "feq_init"));
+    }
+    LB_CUDA(cudaStreamSynchronize(s->stream));
+    s->uploaded = true;
+    s->f_post = false;
+    s->steps = 0;
+    return LBMAN_OK;
+}
+
+int lbman_init_seeded(lbman_solver* s, uint64_t seed, double S0, double sigma) {
+    if (!s) return fail(LBMAN_ERR_ARG, "null solver");
+    LB_TRY(set_device(s));
+    LB_TRY(check_launch(s, s->ops().seeded_init(s->P, seed, S0, sigma, s->rho, s->u[s->ucur], s->q[s->qcur], s->F, s->stream),
+                        "seeded_init"));
+    LB_TRY(check_launch(s, s->ops().feq_init(s->P, s->rho, s->u[s->ucur], s->f[s->fcur], s->stream), "feq_init"));
+    LB_CUDA(cudaStreamSynchronize(s->stream));
+    s->uploaded = true;
+    s->f_post = false;
+    s->steps = 0;
+    return LBMAN_OK;
+}
+
+int lbman_download(lbman_solver* s, double* rho, double* u3, double* q5, double* f15, double* force3) {
+    if (!s) return fail(LBMAN_ERR_ARG, "null solver");
+    if (!s->uploaded) return fail(LBMAN_ERR_STATE, "download before upload");
+    LB_TRY(set_device(s));
+    const int64_t V = s->P.V;
+    if (rho) LB_TRY(stage_out_real(s, s->rho, rho, V));
+    if (u3) for (int k = 0; k < 3; ++k) LB_TRY(stage_out_real(s, vptr(s->u[s->ucur], k * V, s->rbytes), u3 + k * V, V));
+    if (q5) for (int k = 0; k < 5; ++k) LB_TRY(stage_out_real(s, vptr(s->q[s->qcur], k * V, s->rbytes), q5 + k * V, V));
+    if (force3) for (int k = 0; k < 3; ++k) LB_TRY(stage_out_real(s, vptr(s->F, k * V, s->rbytes), force3 + k * V, V));
+    if (f15) {
+        const void* src = s->f[s->fcur];
+        if (s->f_post) {  // stream the stored f* into the spare buffer
+            LB_TRY(check_launch(s, s->ops().stream_only(s->P, s->f[s->fcur], s->f[1 - s->fcur], s->rho, s->stream), "stream_only"));
+            src = s->f[1 - s->fcur];
+        }
+        for (int j = 0; j < 15; ++j) {
+            if (s->prec == LBMAN_FP64) {
+                LB_CUDA(cudaMemcpyAsync(f15 + j * V, vptr((void*)src, j * V, 8), V * 8, cudaMemcpyDeviceToHost, s->stream));
+            } else {
+                LB_TRY(check_launch(s, s->ops().pop_out(s->P, src, s->staging, j, s->stream), "pop_out"));
+                LB_CUDA(cudaMemcpyAsync(f15 + j * V, s->staging, V * 8, cudaMemcpyDeviceToHost, s->stream));
+            }
+        }
+    }
+    LB_CUDA(cudaStreamSynchronize(s->stream));
+    return LBMAN_OK;
+}
+
+static int one_step(lbman_solver* s, bool last) {
+    const bool first = !s->f_post;
+    const Ops& o = s->ops();
+    if (s->kernels == LBMAN_KERNELS_FUSED) {
+        LB_TRY(check_launch(s,
+                            o.fused(s->P, s->shape, first, s->q[s->qcur], s->u[s->ucur], s->q[1 - s->qcur],
+                                    s->u[1 - s->ucur], s->f[s->fcur], s->f[1 - s->fcur], s->rho,
+                                    last ? s->F : nullptr, last, s->stream),
+                            "fused step"));
+        s->qcur ^= 1;
+        s->ucur ^= 1;
+        s->fcur ^= 1;
+    } else {
+        LB_TRY(check_launch(s, o.qforce(s->P, s->shape, s->q[s->qcur], s->u[s->ucur], s->q[1 - s->qcur], s->F, s->stream),
+                            "qforce"));
+        s->qcur ^= 1;
+        LB_TRY(check_launch(s, o.lbm(s->P, first, last, s->f[s->fcur], s->f[1 - s->fcur], s->F, s->rho, s->u[s->ucur], s->stream),
+                            "lbm"));
+        s->fcur ^= 1;
+    }
+    s->f_post = true;
+    ++s->steps;
+    return LBMAN_OK;
+}
+
+int lbman_step(lbman_solver* s, int nsteps) {
+    if (!s || nsteps < 0) return fail(LBMAN_ERR_ARG, "bad arguments");
+    if (!s->uploaded) return fail(LBMAN_ERR_STATE, "step before upload");
+    LB_TRY(set_device(s));
+    for (int n = 0; n < nsteps; ++n) LB_TRY(one_step(s, n == nsteps - 1));
+    return LBMAN_OK;
+}
+
+int lbman_qtensor_step(lbman_solver* s) {
+    if (!s) return fail(LBMAN_ERR_ARG, "null solver");
+    if (!s->uploaded) return fail(LBMAN_ERR_STATE, "step before upload");
+    LB_TRY(set_device(s));
+    LB_TRY(check_launch(s, s->ops().qforce(s->P, s->shape, s->q[s->qcur], s->u[s->ucur], s->q[1 - s->qcur], s->F, s->stream),
+                        "qforce"));
+    s->qcur ^= 1;
+    return LBMAN_OK;
+}
+
+int lbman_lbm_step(lbman_solver* s) {
+    if (!s) return fail(LBMAN_ERR_ARG, "null solver");
+    if (!s->uploaded) return fail(LBMAN_ERR_STATE, "step before upload");
+    LB_TRY(set_device(s));
+    LB_TRY(check_launch(s, s->ops().lbm(s->P, !s->f_post, true, s->f[s->fcur], s->f[1 - s->fcur], s->F, s->rho, s->u[s->ucur], s->stream),
+                        "lbm"));
+    s->fcur ^= 1;
+    s->f_post = true;
+    return LBMAN_OK;
+}
+
+int lbman_reduce(lbman_solver* s, int flags, lbman_diag* out) {
+    if (!s || !out) return fail(LBMAN_ERR_ARG, "null argument");
+    if (!s->uploaded) return fail(LBMAN_ERR_STATE, "reduce before upload");
+    LB_TRY(set_device(s));
+    const int64_t V = s->P.V;
+    const int G = s->red_G;
+    const Ops& o = s->ops();
+    std::memset(out, 0, sizeof(*out));
+    out->defect_faces = -1;
+    if (flags & LBMAN_DIAG_FLOW) {
+        if (!s->upast) {
+            LB_CUDA(cudaMalloc(&s->upast, 3 * V * s->rbytes));
+            LB_CUDA(cudaMemsetAsync(s->upast, 0, 3 * V * s->rbytes, s->stream));
+        }
+        LB_TRY(check_launch(s, o.flow_reduce(s->P, s->rho, s->u[s->ucur], s->upast, s->partials, G, s->stream), "flow_reduce"));
+        LB_TRY(check_launch(s, launch_fold(s->partials, G, 8, 1, s->red_dev, s->stream), "fold"));
+    }
+    if (flags & LBMAN_DIAG_ENERGY) {
+        LB_TRY(check_launch(s, o.energy_reduce(s->P, s->q[s->qcur], s->partials, G, s->stream), "energy_reduce"));
+        LB_TRY(check_launch(s, launch_fold(s->partials, G, 1, 0, s->red_dev + 8, s->stream), "fold"));
+    }
+    const bool defects = (flags & LBMAN_DIAG_DEFECTS) && s->P.nx >= 2 && s->P.ny >= 2 && s->P.nz >= 2;
+    if (defects) {
+        if (!s->dirbuf) LB_CUDA(cudaMalloc(&s->dirbuf, 3 * V * s->rbytes));
+        LB_TRY(check_launch(s, o.director(s->P, s->q[s->qcur], nullptr, s->dirbuf, G, s->stream), "director"));
+        LB_TRY(check_launch(s, o.defect_count(s->P, s->dirbuf, s->partials, G, s->stream), "defect_count"));
+        LB_TRY(check_launch(s, launch_fold(s->partials, G, 1, 0, s->red_dev + 9, s->stream), "fold"));
+    }
+    LB_CUDA(cudaMemcpyAsync(s->red_host, s->red_dev, 10 * sizeof(double), cudaMemcpyDeviceToHost, s->stream));
+    LB_CUDA(cudaStreamSynchronize(s->stream));
+    const double* r = s->red_host;
+    if (flags & LBMAN_DIAG_FLOW) {
+        out->mass = r[0]; out->px = r[1]; out->py = r[2]; out->pz = r[3];
+        out->kinetic_energy = r[4]; out->rel_change_num = r[5]; out->rel_change_den = r[6]; out->umax2 = r[7];
+        out->nan_detected = std::isnan(r[0]) || std::isnan(r[1]) || std::isnan(r[2]) || std::isnan(r[3]);
+    }
+    if (flags & LBMAN_DIAG_ENERGY) out->free_energy = r[8];
+    if (defects) out->defect_faces = (int64_t)std::llround(r[9]);
+    if (out->nan_detected) return fail(LBMAN_ERR_DIVERGED, "NaN in the global mass or momentum");
+    return LBMAN_OK;
+}
+
+int lbman_steps_done(lbman_solver* s, int64_t* steps) {
+    if (!s || !steps) return fail(LBMAN_ERR_ARG, "null argument");
+    *steps = s->steps;
+    return LBMAN_OK;
+}
+
+int lbman_launch_count(lbman_solver* s, int64_t* launches) {
+    if (!s || !launches) return fail(LBMAN_ERR_ARG, "null argument");
+    *launches = s->launches;
+    return LBMAN_OK;
+}
+
+}  // extern "C"

@@ -1,0 +1,237 @@
+// kernels_impl.cuh -- launcher bodies, instantiated per precision by
+// kernels_f64.cu / kernels_f32.cu.
+#pragma once
+
+#include "fused.cuh"
+#include "init.cuh"
+#include "launch.h"
+#include "reduce.cuh"
+
+namespace lbman {
+namespace impl {
+
+inline unsigned blocks_for(int64_t n, int threads) { return (unsigned)((n + threads - 1) / threads); }
+
+inline dim3 qgrid(const SimParams& P, const QTile& T) {
+    return dim3((unsigned)((P.nx + T.tcx - 1) / T.tcx), (unsigned)((P.ny + T.tcy - 1) / T.tcy),
+                (unsigned)((P.nz + T.zc - 1) / T.zc));
+}
+
+template <class R>
+size_t qforce_smem(const QTile& T) {
+    return qforce_smem_bytes(T, sizeof(R));
+}
+
+template <class R>
+cudaError_t qforce(const SimParams& P, const LaunchShape& S, const void* qin, const void* uin, void* qout,
+                   void* Fout, cudaStream_t st) {
+    const size_t smem = qforce_smem<R>(S.tile);
+    if (P.upwind)
+        qforce_kernel<R, true><<<qgrid(P, S.tile), S.qthreads, smem, st>>>(
+            P, S.tile, (const R*)qin, (const R*)uin, (R*)qout, (R*)Fout);
+    else
+        qforce_kernel<R, false><<<qgrid(P, S.tile), S.qthreads, smem, st>>>(
+            P, S.tile, (const R*)qin, (const R*)uin, (R*)qout, (R*)Fout);
+    return cudaGetLastError();
+}
+
+template <class R, class S, bool DEV>
+cudaError_t fused(const SimParams& P, const LaunchShape& L, bool first, const void* qin, const void* uin,
+                  void* qout, void* uout, const void* fin, void* fout, void* rho, void* Fout, bool wr,
+                  cudaStream_t st) {
+    const size_t smem = qforce_smem<R>(L.tile);
+    const dim3 g = qgrid(P, L.tile);
+#define LBMAN_FUSED(UP, FI)                                                                           \
+    fused_kernel<R, S, DEV, UP, FI><<<g, L.qthreads, smem, st>>>(P, L.tile, (const R*)qin,            \
+                                                                 (const R*)uin, (R*)qout, (R*)uout,   \
+                                                                 (const S*)fin, (S*)fout, (R*)rho,    \
+                                                                 (R*)Fout, wr ? 1 : 0)
+    if (P.upwind) { if (first) LBMAN_FUSED(true, true); else LBMAN_FUSED(true, false); }
+    else { if (first) LBMAN_FUSED(false, true); else LBMAN_FUSED(false, false); }
+#undef LBMAN_FUSED
+    return cudaGetLastError();
+}
+
+template <class R, class S, bool DEV>
+cudaError_t lbm(const SimParams& P, bool first, bool wr, const void* fin, void* fout, const void* F,
+                void* rho, void* uout, cudaStream_t st) {
+    const FastDiv dnx = make_fastdiv((uint32_t)P.nx), dnxy = make_fastdiv((uint32_t)P.nxy);
+    const unsigned nb = blocks_for(P.V, 256);
+    if (first)
+        lbm_kernel<R, S, DEV, true><<<nb, 256, 0, st>>>(P, dnx, dnxy, (const S*)fin, (S*)fout, (const R*)F,
+                                                        (R*)rho, (R*)uout, wr ? 1 : 0);
+    else
+        lbm_kernel<R, S, DEV, false><<<nb, 256, 0, st>>>(P, dnx, dnxy, (const S*)fin, (S*)fout, (const R*)F,
+                                                         (R*)rho, (R*)uout, wr ? 1 : 0);
+    return cudaGetLastError();
+}
+
+template <class R, class S>
+cudaError_t stream_only(const SimParams& P, const void* fin, void* fout, const void* rho, cudaStream_t st) {
+    const FastDiv dnx = make_fastdiv((uint32_t)P.nx), dnxy = make_fastdiv((uint32_t)P.nxy);
+    stream_only_kernel<R, S><<<blocks_for(P.V, 256), 256, 0, st>>>(P, dnx, dnxy, (const S*)fin, (S*)fout,
+                                                                   (const R*)rho);
+    return cudaGetLastError();
+}
+
+template <class R, class S, bool DEV>
+cudaError_t feq_init(const SimParams& P, const void* rho, const void* u, void* f, cudaStream_t st) {
+    feq_init_kernel<R, S, DEV><<<blocks_for(P.V, 256), 256, 0, st>>>(P, (const R*)rho, (const R*)u, (S*)f);
+    return cudaGetLastError();
+}
+
+__device__ __forceinline__ void to_s(double v, double* d) { *d = v; }
+__device__ __forceinline__ void to_s(double v, float* d) { *d = (float)v; }
+__device__ __forceinline__ void to_s(double v, __half* d) { *d = __double2half(v); }
+__device__ __forceinline__ double from_s(const double* s) { return *s; }
+__device__ __forceinline__ double from_s(const float* s) { return (double)*s; }
+__device__ __forceinline__ double from_s(const __half* s) { return (double)__half2float(*s); }
+
+template <class T>
+__global__ void to_storage_kernel(const double* __restrict__ src, T* __restrict__ dst, int64_t n, double off) {
+    const int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (i < n) to_s(src[i] - off, dst + i);
+}
+template <class T>
+__global__ void from_storage_kernel(const T* __restrict__ src, double* __restrict__ dst, int64_t n, double off) {
+    const int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (i < n) dst[i] = from_s(src + i) + off;
+}
+
+// Populations of direction dir: host f_i <-> stored value (deviation form
+// subtracts w_i rho0).
+template <class S, bool DEV>
+cudaError_t pop_in(const SimParams& P, const double* src, void* dst, int dir, cudaStream_t st) {
+    const double off = DEV ? w_<double>(dir) * P.kDensity : 0.0;
+    to_storage_kernel<S><<<blocks_for(P.V, 256), 256, 0, st>>>(src, (S*)dst + (int64_t)dir * P.V, P.V, off);
+    return cudaGetLastError();
+}
+template <class S, bool DEV>
+cudaError_t pop_out(const SimParams& P, const void* src, double* dst, int dir, cudaStream_t st) {
+    const double off = DEV ? w_<double>(dir) * P.kDensity : 0.0;
+    from_storage_kernel<S><<<blocks_for(P.V, 256), 256, 0, st>>>((const S*)src + (int64_t)dir * P.V, dst, P.V, off);
+    return cudaGetLastError();
+}
+template <class R>
+cudaError_t real_in(const double* src, void* dst, int64_t n, cudaStream_t st) {
+    to_storage_kernel<R><<<blocks_for(n, 256), 256, 0, st>>>(src, (R*)dst, n, 0.0);
+    return cudaGetLastError();
+}
+template <class R>
+cudaError_t real_out(const void* src, double* dst, int64_t n, cudaStream_t st) {
+    from_storage_kernel<R><<<blocks_for(n, 256), 256, 0, st>>>((const R*)src, dst, n, 0.0);
+    return cudaGetLastError();
+}
+
+template <class R>
+cudaError_t flow_reduce(const SimParams& P, const void* rho, const void* u, void* upast, double* partials, int G,
+                        cudaStream_t st) {
+    flow_reduce_kernel<R><<<G, kRedThreads, 0, st>>>(P, (const R*)rho, (const R*)u, (R*)upast, partials);
+    return cudaGetLastError();
+}
+template <class R>
+cudaError_t energy_reduce(const SimParams& P, const void* q, double* partials, int G, cudaStream_t st) {
+    energy_reduce_kernel<R><<<G, kRedThreads, 0, st>>>(P, (const R*)q, partials);
+    return cudaGetLastError();
+}
+template <class R>
+cudaError_t director(const SimParams& P, const void* q, void* order, void* dir, int G, cudaStream_t st) {
+    director_kernel<R><<<G, kRedThreads, 0, st>>>(P, (const R*)q, (R*)order, (R*)dir);
+    return cudaGetLastError();
+}
+template <class R>
+cudaError_t defect_count(const SimParams& P, const void* dir, double* partials, int G, cudaStream_t st) {
+    defect_count_kernel<R><<<G, kRedThreads, 0, st>>>(P, (const R*)dir, partials);
+    return cudaGetLastError();
+}
+
+template <class R>
+cudaError_t seeded_init(const SimParams& P, uint64_t seed, double S0, double sigma, void* rho, void* u, void* q,
+                        void* F, cudaStream_t st) {
+    const uint64_t key = splitmix64(seed ^ 0x5851f42d4c957f2dULL);
+    seeded_init_kernel<R><<<blocks_for(P.V, 256), 256, 0, st>>>(P, key, S0, sigma, (R*)rho, (R*)u, (R*)q, (R*)F);
+    return cudaGetLastError();
+}
+
+template <class R, class S, bool DEV>
+cudaError_t prepare(size_t max_smem) {
+    const int b = (int)max_smem;
+    cudaError_t e = cudaSuccess;
+#define LBMAN_ATTR(K) \
+    if (e == cudaSuccess) e = cudaFuncSetAttribute(K, cudaFuncAttributeMaxDynamicSharedMemorySize, b)
+    LBMAN_ATTR((qforce_kernel<R, true>));
+    LBMAN_ATTR((qforce_kernel<R, false>));
+    LBMAN_ATTR((fused_kernel<R, S, DEV, true, true>));
+    LBMAN_ATTR((fused_kernel<R, S, DEV, true, false>));
+    LBMAN_ATTR((fused_kernel<R, S, DEV, false, true>));
+    LBMAN_ATTR((fused_kernel<R, S, DEV, false, false>));
+#undef LBMAN_ATTR
+    return e;
+}
+
+}  // namespace impl
+}  // namespace lbman
+
+// Defines the launch_*_SUF functions of launch.h for compute type R,
+// population storage S and deviation flag DEV.
+#define LBMAN_DEFINE_LAUNCHERS(SUF, R, S, DEV)                                                          \
+    namespace lbman {                                                                                   \
+    cudaError_t launch_qforce_##SUF(const SimParams& P, const LaunchShape& L, const void* qin,          \
+                                    const void* uin, void* qout, void* Fout, cudaStream_t st) {        \
+        return impl::qforce<R>(P, L, qin, uin, qout, Fout, st);                                         \
+    }                                                                                                   \
+    cudaError_t launch_fused_##SUF(const SimParams& P, const LaunchShape& L, bool first,                \
+                                   const void* qin, const void* uin, void* qout, void* uout,           \
+                                   const void* fin, void* fout, void* rho, void* Fout, bool wr,        \
+                                   cudaStream_t st) {                                                  \
+        return impl::fused<R, S, DEV>(P, L, first, qin, uin, qout, uout, fin, fout, rho, Fout, wr, st); \
+    }                                                                                                   \
+    cudaError_t launch_lbm_##SUF(const SimParams& P, bool first, bool wr, const void* fin, void* fout,  \
+                                 const void* F, void* rho, void* uout, cudaStream_t st) {              \
+        return impl::lbm<R, S, DEV>(P, first, wr, fin, fout, F, rho, uout, st);                         \
+    }                                                                                                   \
+    cudaError_t launch_stream_only_##SUF(const SimParams& P, const void* fin, void* fout,              \
+                                         const void* rho, cudaStream_t st) {                           \
+        return impl::stream_only<R, S>(P, fin, fout, rho, st);                                          \
+    }                                                                                                   \
+    cudaError_t launch_feq_init_##SUF(const SimParams& P, const void* rho, const void* u, void* f,     \
+                                      cudaStream_t st) {                                               \
+        return impl::feq_init<R, S, DEV>(P, rho, u, f, st);                                             \
+    }                                                                                                   \
+    cudaError_t launch_pop_in_##SUF(const SimParams& P, const double* src, void* dst, int dir,         \
+                                    cudaStream_t st) {                                                 \
+        return impl::pop_in<S, DEV>(P, src, dst, dir, st);                                              \
+    }                                                                                                   \
+    cudaError_t launch_pop_out_##SUF(const SimParams& P, const void* src, double* dst, int dir,        \
+                                     cudaStream_t st) {                                                \
+        return impl::pop_out<S, DEV>(P, src, dst, dir, st);                                             \
+    }                                                                                                   \
+    cudaError_t launch_real_in_##SUF(const double* src, void* dst, int64_t n, cudaStream_t st) {       \
+        return impl::real_in<R>(src, dst, n, st);                                                       \
+    }                                                                                                   \
+    cudaError_t launch_real_out_##SUF(const void* src, double* dst, int64_t n, cudaStream_t st) {      \
+        return impl::real_out<R>(src, dst, n, st);                                                      \
+    }                                                                                                   \
+    cudaError_t launch_flow_reduce_##SUF(const SimParams& P, const void* rho, const void* u,           \
+                                         void* upast, double* partials, int G, cudaStream_t st) {      \
+        return impl::flow_reduce<R>(P, rho, u, upast, partials, G, st);                                 \
+    }                                                                                                   \
+    cudaError_t launch_energy_reduce_##SUF(const SimParams& P, const void* q, double* partials, int G,  \
+                                           cudaStream_t st) {                                          \
+        return impl::energy_reduce<R>(P, q, partials, G, st);                                           \
+    }                                                                                                   \
+    cudaError_t launch_director_##SUF(const SimParams& P, const void* q, void* order, void* dir, int G, \
+                                      cudaStream_t st) {                                               \
+        return impl::director<R>(P, q, order, dir, G, st);                                              \
+    }                                                                                                   \
+    cudaError_t launch_defect_count_##SUF(const SimParams& P, const void* dir, double* partials, int G, \
+                                          cudaStream_t st) {                                           \
+        return impl::defect_count<R>(P, dir, partials, G, st);                                          \
+    }                                                                                                   \
+    cudaError_t launch_seeded_init_##SUF(const SimParams& P, uint64_t seed, double S0, double sigma,    \
+                                         void* rho, void* u, void* q, void* F, cudaStream_t st) {      \
+        return impl::seeded_init<R>(P, seed, S0, sigma, rho, u, q, F, st);                              \
+    }                                                                                                   \
+    size_t qforce_smem_##SUF(const QTile& T) { return impl::qforce_smem<R>(T); }                       \
+    cudaError_t prepare_##SUF(size_t max_smem) { return impl::prepare<R, S, DEV>(max_smem); }           \
+    }

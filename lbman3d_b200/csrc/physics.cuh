@@ -1,0 +1,214 @@
+// physics.cuh -- pointwise Beris-Edwards / D3Q15 physics and the wall ghost
+// rules, templated on the compute type R.
+//
+// The FP64 instantiation is compiled with --fmad=false and keeps the
+// association order of the reference's expressions term for term
+// (src/model.h:102-361, src/physics_helpers.h:69-129,
+// src/boundary_handler.h:112-392), so its results are bitwise equal to the
+// reference CPU solver.  The FP32 instantiation is the same algebra with
+// contraction allowed.
+#pragma once
+
+#include "common.cuh"
+
+namespace lbman {
+
+// First/second differences of one Q component (QDerivs, src/qtensor_types.h:304).
+template <class R>
+struct QD {
+    R dx, dy, dz, lap, d2x, d2y, d2z;
+};
+
+// Neighbour pair for one Q component along one axis.  m_img / p_img are the
+// values stored at the periodic image positions a-1 / a+1 (always present in
+// the staged tile); the rule below picks them, the centre (clamp) or the
+// anchoring ghost exactly like SafeFetchAxisOffset + QAxisGhostPair
+// (src/boundary_handler.h:76-89, 253-282).
+template <class R>
+__device__ __forceinline__ void q_pair(const SimParams& P, int ax, int comp, int a, int n, R m_img,
+                                       R c, R p_img, R& m, R& p) {
+    const int lo = 2 * ax, hi = lo + 1;
+    m = (a == 0 && !P.qper[lo]) ? c : m_img;
+    p = (a == n - 1 && !P.qper[hi]) ? c : p_img;
+    if (!P.qper[lo]) {  // the Lo tag decides whether ghosts apply on this axis
+        if (a == 0) m = P.face[lo].qbc == Q_ANCHORING ? R(2.0) * R(P.face[lo].anchor[comp]) - c : c;
+        if (a == n - 1) p = P.face[hi].qbc == Q_ANCHORING ? R(2.0) * R(P.face[hi].anchor[comp]) - c : c;
+    }
+}
+
+template <class R>
+__device__ __forceinline__ QD<R> q_derivs(R xm, R xp, R ym, R yp, R zm, R zp, R c) {
+    QD<R> d;
+    d.dx = (xp - xm) / R(2.0);
+    d.dy = (yp - ym) / R(2.0);
+    d.dz = (zp - zm) / R(2.0);
+    d.lap = (xm + xp + ym + yp + zm + zp) - R(6.0) * c;
+    d.d2x = (xm + xp) - R(2.0) * c;
+    d.d2y = (ym + yp) - R(2.0) * c;
+    d.d2z = (zm + zp) - R(2.0) * c;
+    return d;
+}
+
+// VelocityGhost / VelocityAxisGradient (src/boundary_handler.h:121-163).
+template <class R>
+__device__ __forceinline__ R v_ghost(const SimParams& P, int face, int comp, R vb, bool normal) {
+    const Face& f = P.face[face];
+    const R wall = f.ubc == U_MOVING ? R(f.uw[comp]) : R(0.0);
+    if (f.ubc == U_SPECULAR) return normal ? (R(2.0) * wall - vb) : vb;
+    return R(2.0) * wall - vb;
+}
+
+template <class R>
+__device__ __forceinline__ R v_grad(const SimParams& P, int ax, int comp, int a, int n, R m_img, R c,
+                                    R p_img, bool normal) {
+    const int lo = 2 * ax, hi = lo + 1;
+    R m = (a == 0 && !P.uper[lo]) ? c : m_img;
+    R p = (a == n - 1 && !P.uper[hi]) ? c : p_img;
+    if (!P.uper[lo]) {
+        if (a == 0) m = v_ghost<R>(P, lo, comp, c, normal);
+        if (a == n - 1) p = v_ghost<R>(P, hi, comp, c, normal);
+    }
+    return (p - m) / R(2.0);
+}
+
+template <class R>
+struct GradU {
+    R ux_x, ux_y, ux_z, uy_x, uy_y, uy_z, uz_x, uz_y;
+};
+
+// AdvectiveAxisTerm / AdvectiveDerivative (src/model.h:60-82).
+template <class R, bool UPWIND>
+__device__ __forceinline__ R adv_axis(R u, R dq, R d2q) {
+    if (UPWIND) {
+        const R au = u < R(0.0) ? -u : u;
+        return u * dq - R(0.5) * au * d2q;
+    }
+    return u * dq;
+}
+template <class R, bool UPWIND>
+__device__ __forceinline__ R adv_deriv(R ux, R uy, R uz, const QD<R>& d) {
+    return adv_axis<R, UPWIND>(ux, d.dx, d.d2x) + adv_axis<R, UPWIND>(uy, d.dy, d.d2y) +
+           adv_axis<R, UPWIND>(uz, d.dz, d.d2z);
+}
+
+// PointwiseStepAndSetupBodyForce (src/model.h:102-342): Q_new, Sigma, tau and
+// the Ericksen force -H:grad Q at one cell.
+template <class R, bool UPWIND>
+__device__ __forceinline__ void pointwise_q(const SimParams& P, const R Q[5], R ux, R uy, R uz,
+                                            const QD<R> d[5], const GradU<R>& g, R qn[5], R sig[5],
+                                            R tau[3], R eric[3]) {
+    const R A = R(P.A), B = R(P.B), C = R(P.C), L = R(P.L), LAMBDA = R(P.LAMBDA),
+            GAMMA = R(P.GAMMA), DT = R(P.DT);
+    const R Qxx = Q[0], Qxy = Q[1], Qxz = Q[2], Qyy = Q[3], Qyz = Q[4];
+
+    const R TrQ2 = R(2.0) * (Qxx * Qxx + Qyy * Qyy + Qxx * Qyy + Qxy * Qxy + Qxz * Qxz + Qyz * Qyz);
+    const R k13 = R(1.0 / 3.0);
+    const R Q2_xx = Qxx * Qxx + Qxy * Qxy + Qxz * Qxz - k13 * TrQ2;
+    const R Q2_xy = Qxx * Qxy + Qxy * Qyy + Qxz * Qyz;
+    const R Q2_xz = Qxy * Qyz - Qxz * Qyy;
+    const R Q2_yy = Qxy * Qxy + Qyy * Qyy + Qyz * Qyz - k13 * TrQ2;
+    const R Q2_yz = Qxy * Qxz - Qyz * Qxx;
+
+    const R Exx = g.ux_x;
+    const R Exy = R(0.5) * (g.ux_y + g.uy_x);
+    const R Exz = R(0.5) * (g.ux_z + g.uz_x);
+    const R Eyy = g.uy_y;
+    const R Eyz = R(0.5) * (g.uy_z + g.uz_y);
+    const R Wxy = R(0.5) * (g.ux_y - g.uy_x);
+    const R Wxz = R(0.5) * (g.ux_z - g.uz_x);
+    const R Wyz = R(0.5) * (g.uy_z - g.uz_y);
+
+    const R adv_xx = -adv_deriv<R, UPWIND>(ux, uy, uz, d[0]);
+    const R adv_xy = -adv_deriv<R, UPWIND>(ux, uy, uz, d[1]);
+    const R adv_xz = -adv_deriv<R, UPWIND>(ux, uy, uz, d[2]);
+    const R adv_yy = -adv_deriv<R, UPWIND>(ux, uy, uz, d[3]);
+    const R adv_yz = -adv_deriv<R, UPWIND>(ux, uy, uz, d[4]);
+
+    const R cor_xx = R(2.0) * (Qxy * Wxy + Qxz * Wxz);
+    const R cor_xy = -Qxx * Wxy + Qxz * Wyz + Qyy * Wxy + Qyz * Wxz;
+    const R cor_xz = R(-2.0) * Qxx * Wxz - Qxy * Wyz - Qyy * Wxz + Qyz * Wxy;
+    const R cor_yy = R(2.0) * (-Qxy * Wxy + Qyz * Wyz);
+    const R cor_yz = -Qxx * Wyz - Qxy * Wxz - Qxz * Wxy - R(2.0) * Qyy * Wyz;
+
+    const R k23 = R(2.0 / 3.0);
+    const R tr_QE = (R(2.0) * Exx + Eyy) * Qxx + (R(2.0) * Exy) * Qxy + (R(2.0) * Exz) * Qxz +
+                    (Exx + R(2.0) * Eyy) * Qyy + R(2.0) * Eyz * Qyz;
+    const R aln2_xx = R(2.0) * (Exx * Qxx + Exy * Qxy + Exz * Qxz) - k23 * tr_QE;
+    const R aln2_xy = Exy * Qxx + Eyy * Qxy + Eyz * Qxz + Qxy * Exx + Qyy * Exy + Qyz * Exz;
+    const R aln2_xz =
+        Exz * Qxx + Eyz * Qxy + (-Exx - Eyy) * Qxz + Qxz * Exx + Qyz * Exy + (-Qxx - Qyy) * Exz;
+    const R aln2_yy = R(2.0) * (Exy * Qxy + Eyy * Qyy + Eyz * Qyz) - k23 * tr_QE;
+    const R aln2_yz =
+        Exz * Qxy + Eyz * Qyy + (-Exx - Eyy) * Qyz + Qxz * Exy + Qyz * Eyy + (-Qxx - Qyy) * Eyz;
+    const R aln3_xx = R(-2.0) * tr_QE * Qxx;
+    const R aln3_xy = R(-2.0) * tr_QE * Qxy;
+    const R aln3_xz = R(-2.0) * tr_QE * Qxz;
+    const R aln3_yy = R(-2.0) * tr_QE * Qyy;
+    const R aln3_yz = R(-2.0) * tr_QE * Qyz;
+
+    const R ld = A + C * TrQ2;
+    const R Hxx = L * d[0].lap - ld * Qxx - B * Q2_xx;
+    const R Hxy = L * d[1].lap - ld * Qxy - B * Q2_xy;
+    const R Hxz = L * d[2].lap - ld * Qxz - B * Q2_xz;
+    const R Hyy = L * d[3].lap - ld * Qyy - B * Q2_yy;
+    const R Hyz = L * d[4].lap - ld * Qyz - B * Q2_yz;
+
+    eric[0] = R(-2.0) * (Hxx * d[0].dx + Hxy * d[1].dx + Hxz * d[2].dx + Hyy * d[3].dx + Hyz * d[4].dx) -
+              Hxx * d[3].dx - Hyy * d[0].dx;
+    eric[1] = R(-2.0) * (Hxx * d[0].dy + Hxy * d[1].dy + Hxz * d[2].dy + Hyy * d[3].dy + Hyz * d[4].dy) -
+              Hxx * d[3].dy - Hyy * d[0].dy;
+    eric[2] = R(-2.0) * (Hxx * d[0].dz + Hxy * d[1].dz + Hxz * d[2].dz + Hyy * d[3].dz + Hyz * d[4].dz) -
+              Hxx * d[3].dz - Hyy * d[0].dz;
+
+    const R tr_QH = (R(2.0) * Hxx + Hyy) * Qxx + (R(2.0) * Hxy) * Qxy + (R(2.0) * Hxz) * Qxz +
+                    (Hxx + R(2.0) * Hyy) * Qyy + R(2.0) * Hyz * Qyz;
+    const R QHxx = R(2.0) * (Hxx * Qxx + Hxy * Qxy + Hxz * Qxz) - k23 * tr_QH;
+    const R QHxy = Hxy * Qxx + Hyy * Qxy + Hyz * Qxz + Qxy * Hxx + Qyy * Hxy + Qyz * Hxz;
+    const R QHxz =
+        Hxz * Qxx + Hyz * Qxy + (-Hxx - Hyy) * Qxz + Qxz * Hxx + Qyz * Hxy + (-Qxx - Qyy) * Hxz;
+    const R QHyy = R(2.0) * (Hxy * Qxy + Hyy * Qyy + Hyz * Qyz) - k23 * tr_QH;
+    const R QHyz =
+        Hxz * Qxy + Hyz * Qyy + (-Hxx - Hyy) * Qyz + Qxz * Hxy + Qyz * Hyy + (-Qxx - Qyy) * Hyz;
+
+    tau[0] = (Hxy * Qxx + Hyy * Qxy + Hyz * Qxz) - (Qxy * Hxx + Qyy * Hxy + Qyz * Hxz);
+    tau[1] = (Hxz * Qxx + Hyz * Qxy + (-Hxx - Hyy) * Qxz) - (Qxz * Hxx + Qyz * Hxy + (-Qxx - Qyy) * Hxz);
+    tau[2] = (Hxz * Qxy + Hyz * Qyy + (-Hxx - Hyy) * Qyz) - (Qxz * Hxy + Qyz * Hyy + (-Qxx - Qyy) * Hyz);
+
+    const R mk23L = -k23 * LAMBDA;
+    const R twoL = R(2.0) * LAMBDA;
+    sig[0] = mk23L * Hxx - LAMBDA * QHxx + twoL * tr_QH * Qxx;
+    sig[1] = mk23L * Hxy - LAMBDA * QHxy + twoL * tr_QH * Qxy;
+    sig[2] = mk23L * Hxz - LAMBDA * QHxz + twoL * tr_QH * Qxz;
+    sig[3] = mk23L * Hyy - LAMBDA * QHyy + twoL * tr_QH * Qyy;
+    sig[4] = mk23L * Hyz - LAMBDA * QHyz + twoL * tr_QH * Qyz;
+
+    qn[0] = Qxx + DT * (adv_xx + cor_xx + LAMBDA * (k23 * Exx + aln2_xx + aln3_xx) + GAMMA * Hxx);
+    qn[1] = Qxy + DT * (adv_xy + cor_xy + LAMBDA * (k23 * Exy + aln2_xy + aln3_xy) + GAMMA * Hxy);
+    qn[2] = Qxz + DT * (adv_xz + cor_xz + LAMBDA * (k23 * Exz + aln2_xz + aln3_xz) + GAMMA * Hxz);
+    qn[3] = Qyy + DT * (adv_yy + cor_yy + LAMBDA * (k23 * Eyy + aln2_yy + aln3_yy) + GAMMA * Hyy);
+    qn[4] = Qyz + DT * (adv_yz + cor_yz + LAMBDA * (k23 * Eyz + aln2_yz + aln3_yz) + GAMMA * Hyz);
+}
+
+// PointwiseSetActiveStressAndComputeBodyForce + PassiveStressDivergence sums
+// (src/model.h:344-361, src/boundary_handler.h:379-391): the force added to
+// the Ericksen seed.  dS[axis][comp] are the centred differences of the 5
+// Sigma components, dT[axis][comp] of the 3 tau components.
+template <class R>
+__device__ __forceinline__ void active_passive_force(const SimParams& P, const R dQ[5][3],
+                                                     const R dS[3][5], const R dT[3][3], R ux, R uy,
+                                                     R uz, const R eric[3], R F[3]) {
+    const R ALPHA = R(P.ALPHA), MU = R(P.MU);
+    // f_x = d_x S_xx + d_y(S_xy + T_xy) + d_z(S_xz + T_xz), ... (row convention)
+    const R dz_Szz = -(dS[2][0] + dS[2][3]);
+    const R pdx = dS[0][0] + (dS[1][1] + dT[1][0]) + (dS[2][2] + dT[2][1]);
+    const R pdy = (dS[0][1] - dT[0][0]) + dS[1][3] + (dS[2][4] + dT[2][2]);
+    const R pdz = (dS[0][2] - dT[0][1]) + (dS[1][4] - dT[1][2]) + dz_Szz;
+    const R fx = -ALPHA * (dQ[0][0] + dQ[1][1] + dQ[2][2]) + pdx - MU * ux;
+    const R fy = -ALPHA * (dQ[1][0] + dQ[3][1] + dQ[4][2]) + pdy - MU * uy;
+    const R fz = -ALPHA * (dQ[2][0] + dQ[4][1] - dQ[0][2] - dQ[3][2]) + pdz - MU * uz;
+    F[0] = eric[0] + fx;
+    F[1] = eric[1] + fy;
+    F[2] = eric[2] + fz;
+}
+
+}  // namespace lbman

@@ -1,0 +1,242 @@
+"""GPU solver objects with the reference's interface, over the C ABI.
+
+* :class:`DeviceFields` / :class:`DeviceSolver` mirror src/device_fields.h
+  and src/device_solver.h: device-resident state, ``Initialize`` (upload),
+  ``QTensorStep``, ``LBMStep``, ``CopyToHost``.
+* :class:`LbmSolver` / :class:`QTensorSolver` mirror src/lbm_solver.h and
+  src/qtensor_solver.h: they operate on host ``FluidFields`` /
+  ``QTensorFields`` and run each call on the GPU (upload, step, download).
+* :class:`Simulation` is a device-resident convenience handle used by the
+  tests and the benchmark: arrays in, arrays out, ``step(n)``, ``reduce()``.
+
+Every call goes to liblbman3d_b200.so; there is no CPU path.
+"""
+from __future__ import annotations
+
+import ctypes as C
+
+import numpy as np
+
+from . import _native as N
+from .boundary import BCConfig, SimBC
+from .fields import FluidFields, LocalGrid, QTensorFields
+from .params import Params, Precision
+
+
+def InitializeComputeBackend(device: int = 0) -> str:
+    """Device description (src/device_fields.h:21)."""
+    buf = C.create_string_buffer(2048)
+    N.check(N.lib().lbman_device_info(device, buf, len(buf)))
+    return buf.value.decode()
+
+
+def make_config(params: Params, bc: BCConfig, precision: int = Precision.FP64,
+                kernels: int = N.KERNELS_AUTO, device: int = 0, tile=None) -> N.lbman_config:
+    cfg = N.lbman_config()
+    N.check(N.lib().lbman_config_init(C.byref(cfg)))
+    cfg.nx, cfg.ny, cfg.nz = params.nx, params.ny, params.nz
+    for k in ("DT", "kDensity", "TAUF", "L", "A", "B", "C", "LAMBDA", "GAMMA", "ALPHA", "MU"):
+        setattr(cfg, k, float(getattr(params, k)))
+    cfg.advection = int(params.kQAdvection)
+    for i, w in enumerate(bc.faces()):
+        cfg.face[i] = w.lower()
+    cfg.precision = int(precision)
+    cfg.kernels = int(kernels)
+    cfg.device = int(device)
+    if tile:
+        cfg.tile_x, cfg.tile_y, cfg.zchunk, cfg.threads = (list(tile) + [0, 0, 0, 0])[:4]
+    return cfg
+
+
+class Simulation:
+    """One device-resident box.  Host arrays follow the C ABI layout: u is 3
+    blocks of V, q 5 blocks, f 15 direction-major blocks, all float64."""
+
+    def __init__(self, params: Params, bc: BCConfig = None, precision: int = Precision.FP64,
+                 kernels: int = N.KERNELS_AUTO, device: int = 0, tile=None):
+        self.params = params
+        self.bc = bc if bc is not None else SimBC()
+        self.precision = precision
+        self.cfg = make_config(params, self.bc, precision, kernels, device, tile)
+        h = C.c_void_p()
+        N.check(N.lib().lbman_create(C.byref(self.cfg), C.byref(h)))
+        self._h = h
+
+    @property
+    def handle(self):
+        return self._h
+
+    @property
+    def V(self):
+        return self.params.V
+
+    def close(self):
+        if getattr(self, "_h", None):
+            N.lib().lbman_destroy(self._h)
+            self._h = None
+
+    def __del__(self):
+        self.close()
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *a):
+        self.close()
+
+    def upload(self, rho, u, q, f=None, force=None):
+        c = lambda a: None if a is None else np.ascontiguousarray(a, dtype=np.float64)
+        rho, u, q, f, force = c(rho), c(u), c(q), c(f), c(force)
+        V = self.V
+        for name, a, n in (("rho", rho, V), ("u", u, 3 * V), ("q", q, 5 * V), ("f", f, 15 * V),
+                           ("force", force, 3 * V)):
+            if a is not None and a.size != n:
+                raise ValueError(f"{name} must have {n} values, got {a.size}")
+        N.check(N.lib().lbman_upload(self._h, N.dptr(rho), N.dptr(u), N.dptr(q), N.dptr(f), N.dptr(force)))
+
+    def init_seeded(self, seed: int, S0: float, sigma: float = 1e-3):
+        N.check(N.lib().lbman_init_seeded(self._h, int(seed), float(S0), float(sigma)))
+
+    def download(self, f=False, force=False):
+        V = self.V
+        out = dict(rho=np.empty(V), u=np.empty(3 * V), q=np.empty(5 * V))
+        if f:
+            out["f"] = np.empty(15 * V)
+        if force:
+            out["force"] = np.empty(3 * V)
+        N.check(N.lib().lbman_download(self._h, N.dptr(out["rho"]), N.dptr(out["u"]), N.dptr(out["q"]),
+                                       N.dptr(out.get("f")), N.dptr(out.get("force"))))
+        return out
+
+    def step(self, n: int = 1):
+        N.check(N.lib().lbman_step(self._h, int(n)))
+
+    def qtensor_step(self):
+        N.check(N.lib().lbman_qtensor_step(self._h))
+
+    def lbm_step(self):
+        N.check(N.lib().lbman_lbm_step(self._h))
+
+    def synchronize(self):
+        N.check(N.lib().lbman_synchronize(self._h))
+
+    def set_stream(self, stream_ptr: int):
+        N.check(N.lib().lbman_set_stream(self._h, C.c_void_p(stream_ptr)))
+
+    def reduce(self, flags: int = N.DIAG_ALL, raise_on_nan: bool = True):
+        d = N.lbman_diag()
+        st = N.lib().lbman_reduce(self._h, int(flags), C.byref(d))
+        if st != N.OK and not (st == N.ERR_DIVERGED and not raise_on_nan):
+            N.check(st)
+        return {k: getattr(d, k) for k, _ in N.lbman_diag._fields_}
+
+    def launch_count(self) -> int:
+        v = C.c_int64()
+        N.check(N.lib().lbman_launch_count(self._h, C.byref(v)))
+        return v.value
+
+    def steps_done(self) -> int:
+        v = C.c_int64()
+        N.check(N.lib().lbman_steps_done(self._h, C.byref(v)))
+        return v.value
+
+
+class DeviceFields:
+    """Device-resident fields (src/device_fields.h:23-56)."""
+
+    def __init__(self, grid: LocalGrid, params: Params, bc: BCConfig = None,
+                 precision: int = Precision.FP64, kernels: int = N.KERNELS_AUTO, device: int = 0):
+        self.grid = grid
+        self.sim = Simulation(params, bc, precision, kernels, device)
+
+    def Initialize(self, ff: FluidFields, qf: QTensorFields):
+        """Upload populations, body force, density, velocity and Q
+        (src/cuda/device_fields.cu:79-115; the AoS->SoA transpose of f is done
+        here as there).  Unlike the reference, rho and u are uploaded too, so
+        the first Q step sees the host velocity as the CPU path does."""
+        self.sim.upload(ff.rho, ff.u3(), qf.q5(), ff.f_soa(), ff.force3())
+
+    def CopyToHost(self, ff: FluidFields, qf: QTensorFields):
+        """rho, u and Q back to the host (src/cuda/device_fields.cu:118-127)."""
+        out = self.sim.download()
+        V = self.grid.Volume()
+        ff.rho[:] = out["rho"]
+        ff.ux[:], ff.uy[:], ff.uz[:] = out["u"][:V], out["u"][V:2 * V], out["u"][2 * V:]
+        qf.set_q5(out["q"])
+
+
+class DeviceSolver:
+    """DeviceSolver<BC> (src/device_solver.h:10-17).  The BC lives in the
+    DeviceFields' configuration, so the solver itself is stateless."""
+
+    def __init__(self, bc: BCConfig = None):
+        self.bc = bc
+
+    def Initialize(self, df: DeviceFields):
+        pass  # lattice tables are compile-time constants of the kernels
+
+    def QTensorStep(self, df: DeviceFields):
+        df.sim.qtensor_step()
+
+    def LBMStep(self, df: DeviceFields):
+        df.sim.lbm_step()
+
+    def Step(self, df: DeviceFields):
+        df.sim.step(1)
+
+
+class LbmSolver:
+    """LbmSolver<BC> on host fields (src/lbm_solver.h:12-21), each call run on
+    the GPU: upload, step, download."""
+
+    def __init__(self, bc: BCConfig, params: Params, precision: int = Precision.FP64, device: int = 0):
+        self.bc, self.params = bc, params
+        self.sim = Simulation(params, bc, precision, N.KERNELS_SPLIT, device)
+
+    def Initialize(self, ff: FluidFields):
+        """f = f_eq(rho, u) (src/lbm_solver.tpp:35-62)."""
+        V = self.params.V
+        self.sim.upload(ff.rho, ff.u3(), np.zeros(5 * V))
+        ff.set_f_soa(self.sim.download(f=True)["f"])
+
+    def LatticeBoltzmannStep(self, ff: FluidFields):
+        V = self.params.V
+        self.sim.upload(ff.rho, ff.u3(), np.zeros(5 * V), ff.f_soa(), ff.force3())
+        self.sim.lbm_step()
+        out = self.sim.download(f=True)
+        ff.set_f_soa(out["f"])
+        ff.rho[:] = out["rho"]
+        ff.ux[:], ff.uy[:], ff.uz[:] = out["u"][:V], out["u"][V:2 * V], out["u"][2 * V:]
+
+
+class QTensorSolver:
+    """QTensorSolver<BC> on host fields (src/qtensor_solver.h:23-52).  Step =
+    StepAndSetupBodyForce + SetActiveStressAndComputeBodyForce in one GPU pass;
+    like the reference's GPU path, subclass overrides of the activity model
+    are not consulted on the device."""
+
+    def __init__(self, bc: BCConfig, params: Params, precision: int = Precision.FP64, device: int = 0):
+        self.bc, self.params = bc, params
+        self.sim = Simulation(params, bc, precision, N.KERNELS_SPLIT, device)
+
+    def Initialize(self, qf: QTensorFields, seed: int = 0):
+        """Uniform director along z at S_eq plus uniform noise of amplitude NOISE
+        (src/qtensor_solver.tpp:14-48), seeded here for reproducibility."""
+        from .params import EquilibriumScalarOrder
+        rng = np.random.default_rng(seed)
+        s_eq = EquilibriumScalarOrder(self.params)
+        V, nz = self.params.V, self.params.NOISE
+        qf.qxx[:] = -s_eq / 3.0 + rng.uniform(-nz, nz, V)
+        qf.qxy[:] = rng.uniform(-nz, nz, V)
+        qf.qxz[:] = rng.uniform(-nz, nz, V)
+        qf.qyy[:] = -s_eq / 3.0 + rng.uniform(-nz, nz, V)
+        qf.qyz[:] = rng.uniform(-nz, nz, V)
+
+    def Step(self, qf: QTensorFields, ff: FluidFields):
+        V = self.params.V
+        self.sim.upload(ff.rho, ff.u3(), qf.q5())
+        self.sim.qtensor_step()
+        out = self.sim.download(force=True)
+        qf.set_q5(out["q"])
+        F = out["force"]
+        ff.fx[:], ff.fy[:], ff.fz[:] = F[:V], F[V:2 * V], F[2 * V:]
