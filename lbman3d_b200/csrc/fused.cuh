@@ -25,7 +25,7 @@ __global__ void __launch_bounds__(512) fused_kernel(SimParams P, QTile T, const 
                                                     R* __restrict__ Fout, int write_rho_all) {
     extern __shared__ __align__(16) unsigned char smem_raw[];
     R* QU = reinterpret_cast<R*>(smem_raw);
-    R* Bs = QU + 3 * 8 * (T.tcx + 4) * (T.tcy + 4);
+    R* Bs = QU + qf_qu_elems<R>(T);
     const int64_t V = P.V;
     qf_march<R, UPWIND>(P, T, qin, uin, QU, Bs, [&](int x0, int y0, int z0, int zc) {
         qf_force_plane<R>(P, T, x0, y0, z0, zc, QU, Bs,

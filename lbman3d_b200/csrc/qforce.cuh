@@ -24,15 +24,30 @@
 
 namespace lbman {
 
+// Ring slots: results (B) keep 3 planes, staged Q/u keep 4 (one is in flight).
 __device__ __forceinline__ int ring3(int z, int z0) { return (z - z0 + 6) % 3; }
+__device__ __forceinline__ int ring4(int z, int z0) { return (z - z0 + 8) & 3; }
 
+// Asynchronous global->shared copies (cp.async, completion via wait_all).
+__device__ __forceinline__ void cp_async(float* s, const float* g) {
+    asm volatile("cp.async.ca.shared.global [%0], [%1], 4;\n" ::"r"((unsigned)__cvta_generic_to_shared(s)),
+                 "l"(g));
+}
+__device__ __forceinline__ void cp_async(double* s, const double* g) {
+    asm volatile("cp.async.ca.shared.global [%0], [%1], 8;\n" ::"r"((unsigned)__cvta_generic_to_shared(s)),
+                 "l"(g));
+}
+__device__ __forceinline__ void cp_async_wait_all() { asm volatile("cp.async.wait_all;\n" ::: "memory"); }
+
+// Issue the copies of plane zg (Q then u, tile + 2-cell halo, periodic wrap)
+// into its ring slot.  Completes at the next cp_async_wait_all().
 template <class R>
 __device__ __forceinline__ void qf_load_plane(const SimParams& P, const QTile& T, int x0, int y0,
                                               int z0, int zg, const R* __restrict__ qin,
                                               const R* __restrict__ uin, R* QU) {
     const int uxw = T.tcx + 4, uyw = T.tcy + 4, nQU = uxw * uyw;
     const int zw = wrap_coord(zg, P.nz);
-    R* dst = QU + ring3(zg, z0) * 8 * nQU;
+    R* dst = QU + ring4(zg, z0) * 8 * nQU;
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, nwarp = blockDim.x >> 5;
     const int64_t zoff = (int64_t)zw * P.nxy;
     for (int row = warp; row < 8 * uyw; row += nwarp) {
@@ -41,7 +56,7 @@ __device__ __forceinline__ void qf_load_plane(const SimParams& P, const QTile& T
         const R* src = (var < 5 ? qin + (int64_t)var * P.V : uin + (int64_t)(var - 5) * P.V) + zoff +
                        (int64_t)gy * P.nx;
         R* d = dst + var * nQU + ly * uxw;
-        for (int lx = lane; lx < uxw; lx += 32) d[lx] = __ldg(src + wrap_coord(x0 - 2 + lx, P.nx));
+        for (int lx = lane; lx < uxw; lx += 32) cp_async(d + lx, src + wrap_coord(x0 - 2 + lx, P.nx));
     }
 }
 
@@ -50,9 +65,9 @@ __device__ __forceinline__ void qf_compute_plane(const SimParams& P, const QTile
                                                  int z0, int zb, const R* QU, R* Bs) {
     const int uxw = T.tcx + 4, uyw = T.tcy + 4, nQU = uxw * uyw;
     const int bxw = T.tcx + 2, byw = T.tcy + 2, nB = bxw * byw;
-    const R* Qc = QU + ring3(zb, z0) * 8 * nQU;
-    const R* Qm = QU + ring3(zb - 1, z0) * 8 * nQU;
-    const R* Qp = QU + ring3(zb + 1, z0) * 8 * nQU;
+    const R* Qc = QU + ring4(zb, z0) * 8 * nQU;
+    const R* Qm = QU + ring4(zb - 1, z0) * 8 * nQU;
+    const R* Qp = QU + ring4(zb + 1, z0) * 8 * nQU;
     R* Bd = Bs + ring3(zb, z0) * 16 * nB;
     const int az = wrap_coord(zb, P.nz);
     for (int p = threadIdx.x; p < nB; p += blockDim.x) {
@@ -109,7 +124,7 @@ __device__ __forceinline__ void qf_force_plane(const SimParams& P, const QTile& 
     const R* B0 = Bs + ring3(zc, z0) * 16 * nB;
     const R* Bm = Bs + ring3(zc - 1, z0) * 16 * nB;
     const R* Bp = Bs + ring3(zc + 1, z0) * 16 * nB;
-    const R* U0 = QU + ring3(zc, z0) * 8 * nQU;
+    const R* U0 = QU + ring4(zc, z0) * 8 * nQU;
     const int ntile = T.tcx * T.tcy;
     for (int p = threadIdx.x; p < ntile; p += blockDim.x) {
         const int lcy = p / T.tcx, lcx = p - lcy * T.tcx;
@@ -160,7 +175,9 @@ __device__ __forceinline__ void qf_force_plane(const SimParams& P, const QTile& 
 }
 
 // Marches a block through its z chunk; PlaneOut is called once per output
-// plane after the staged planes are complete.
+// plane after the staged planes are complete.  The copy of plane zc+3 is in
+// flight while planes zc+1 (results) and zc (force, output) are computed, so
+// the global-memory latency of the staging is hidden behind the arithmetic.
 template <class R, bool UPWIND, class PlaneOut>
 __device__ __forceinline__ void qf_march(const SimParams& P, const QTile& T,
                                          const R* __restrict__ qin, const R* __restrict__ uin,
@@ -169,23 +186,29 @@ __device__ __forceinline__ void qf_march(const SimParams& P, const QTile& T,
     const int z0 = blockIdx.z * T.zc;
     if (z0 >= P.nz) return;
     const int z1 = min(z0 + T.zc, P.nz);
-    qf_load_plane<R>(P, T, x0, y0, z0, z0 - 2, qin, uin, QU);
-    qf_load_plane<R>(P, T, x0, y0, z0, z0 - 1, qin, uin, QU);
-    qf_load_plane<R>(P, T, x0, y0, z0, z0, qin, uin, QU);
+    for (int z = z0 - 2; z <= z0 + 1; ++z) qf_load_plane<R>(P, T, x0, y0, z0, z, qin, uin, QU);
+    cp_async_wait_all();
     __syncthreads();
     qf_compute_plane<R, UPWIND>(P, T, x0, y0, z0, z0 - 1, QU, Bs);
-    __syncthreads();
-    qf_load_plane<R>(P, T, x0, y0, z0, z0 + 1, qin, uin, QU);
-    __syncthreads();
     qf_compute_plane<R, UPWIND>(P, T, x0, y0, z0, z0, QU, Bs);
+    __syncthreads();  // slot of z0-2 is free again
+    qf_load_plane<R>(P, T, x0, y0, z0, z0 + 2, qin, uin, QU);
+    cp_async_wait_all();
+    __syncthreads();
     for (int zc = z0; zc < z1; ++zc) {
-        __syncthreads();
-        qf_load_plane<R>(P, T, x0, y0, z0, zc + 2, qin, uin, QU);
-        __syncthreads();
+        // slot of zc-1 was last read by the previous iteration (before its final barrier)
+        if (zc + 1 < z1) qf_load_plane<R>(P, T, x0, y0, z0, zc + 3, qin, uin, QU);
         qf_compute_plane<R, UPWIND>(P, T, x0, y0, z0, zc + 1, QU, Bs);
         __syncthreads();
         plane_out(x0, y0, z0, zc);
+        cp_async_wait_all();
+        __syncthreads();
     }
+}
+
+template <class R>
+__host__ __device__ inline int qf_qu_elems(const QTile& T) {
+    return 4 * 8 * (T.tcx + 4) * (T.tcy + 4);
 }
 
 template <class R, bool UPWIND>
@@ -194,7 +217,7 @@ __global__ void __launch_bounds__(512) qforce_kernel(SimParams P, QTile T, const
                                                      R* __restrict__ Fout) {
     extern __shared__ __align__(16) unsigned char smem_raw[];
     R* QU = reinterpret_cast<R*>(smem_raw);
-    R* Bs = QU + 3 * 8 * (T.tcx + 4) * (T.tcy + 4);
+    R* Bs = QU + qf_qu_elems<R>(T);
     const int64_t V = P.V;
     qf_march<R, UPWIND>(P, T, qin, uin, QU, Bs, [&](int x0, int y0, int z0, int zc) {
         qf_force_plane<R>(P, T, x0, y0, z0, zc, QU, Bs,
@@ -208,7 +231,7 @@ __global__ void __launch_bounds__(512) qforce_kernel(SimParams P, QTile T, const
 }
 
 inline size_t qforce_smem_bytes(const QTile& T, size_t real_bytes) {
-    return real_bytes * (size_t)(3 * 8 * (T.tcx + 4) * (T.tcy + 4) + 3 * 16 * (T.tcx + 2) * (T.tcy + 2));
+    return real_bytes * (size_t)(4 * 8 * (T.tcx + 4) * (T.tcy + 4) + 3 * 16 * (T.tcx + 2) * (T.tcy + 2));
 }
 
 }  // namespace lbman
