@@ -154,6 +154,34 @@ int lbman_lbm_step(lbman_solver* s);
  * when the mass or momentum is NaN, as SimIO::Log returns false.            */
 int lbman_reduce(lbman_solver* s, int flags, lbman_diag* out);
 
+/* Flow diagnostics without any device allocation.  No counterpart in the
+ * reference: it is an addition for callers that cannot call cudaMalloc --
+ * a host framework whose allocator already holds (nearly) all device memory,
+ * or a stepping loop that must not allocate or free because cudaFree
+ * synchronises the whole device.
+ *
+ * Computes what lbman_reduce(LBMAN_DIAG_FLOW) computes (mass, momentum,
+ * kinetic energy, relative change against upast3, max |u|^2, NaN check) over
+ * caller-owned device fields: rho[ncells] and u3[3*ncells] (double when
+ * precision is LBMAN_FP64, float when LBMAN_FP32), upast3[3*ncells] of the same
+ * type, read and then overwritten with u3.  Work is issued on cuda_stream
+ * (NULL: the legacy default stream) on the current device, and the call
+ * returns after the result is copied into *out.
+ *
+ * Scratch comes from a fixed array inside the library (partial sums of at
+ * most LBMAN_NOALLOC_MAX_BLOCKS blocks, about 76 KB per device, held by every
+ * GPU that loads the library until the process exits).  The first call on a
+ * device looks up that array's device address; make that first call before
+ * any stream capture.  All calls share the array: calls whose GPU work
+ * overlaps (other streams or threads, same device) race and corrupt each
+ * other's results; serialise them.  ncells above LBMAN_NOALLOC_MAX_CELLS is
+ * rejected with LBMAN_ERR_ARG.  Allocates nothing: no cudaMalloc, no
+ * cudaFree, no allocating library call.                                     */
+#define LBMAN_NOALLOC_MAX_BLOCKS 1184
+#define LBMAN_NOALLOC_MAX_CELLS 2147483647LL
+int lbman_flow_reduce_noalloc(int64_t ncells, int precision, const void* rho, const void* u3,
+                              void* upast3, void* cuda_stream, lbman_diag* out);
+
 /* Steps completed since the last upload. */
 int lbman_steps_done(lbman_solver* s, int64_t* steps);
 /* Kernel launches issued by this solver since creation (instrumentation).  */

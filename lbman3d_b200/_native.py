@@ -77,6 +77,8 @@ PROTOTYPES = [
     ("lbman_reduce", C.c_int, [C.c_void_p, C.c_int, C.POINTER(lbman_diag)]),
     ("lbman_steps_done", C.c_int, [C.c_void_p, C.POINTER(C.c_int64)]),
     ("lbman_launch_count", C.c_int, [C.c_void_p, C.POINTER(C.c_int64)]),
+    ("lbman_flow_reduce_noalloc", C.c_int,
+     [C.c_int64, C.c_int, C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p, C.POINTER(lbman_diag)]),
 ]
 
 

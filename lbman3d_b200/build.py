@@ -33,6 +33,7 @@ UNITS = {
     "kernels_f32.cu": [],
     "kernels_ens.cu": [],
     "api.cu": [],
+    "noalloc.cu": [],
 }
 
 

@@ -93,6 +93,11 @@ void anchored_q(const lbman_face& f, double out[5]) {
 
 }  // namespace
 
+namespace lbman {
+// Error message for lbman_last_error() from other translation units.
+void set_last_error(const char* msg) { g_err = msg; }
+}  // namespace lbman
+
 struct lbman_solver {
     lbman_config cfg;
     SimParams P;
