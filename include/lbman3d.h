@@ -182,6 +182,55 @@ int lbman_reduce(lbman_solver* s, int flags, lbman_diag* out);
 int lbman_flow_reduce_noalloc(int64_t ncells, int precision, const void* rho, const void* u3,
                               void* upast3, void* cuda_stream, lbman_diag* out);
 
+/* Launch shape of the time step: kernel organisation and z-marching tile.   */
+typedef struct lbman_shape {
+    int kernels;              /* LBMAN_KERNELS_SPLIT / LBMAN_KERNELS_FUSED     */
+    int tile_x, tile_y;       /* cells per x-y plane of one block             */
+    int zchunk;               /* z planes marched by one block                */
+    int threads;              /* threads per block (set by the tile)          */
+    double ms_per_step;       /* measured by lbman_autotune, else 0           */
+} lbman_shape;
+
+int lbman_get_shape(lbman_solver* s, lbman_shape* out);
+/* Select a shape (tile_x x tile_y must be one of the compiled tiles: 30x6,
+ * 32x6, 14x14, and for FP32/FP16 also 30x14, 62x6; zchunk >= 1).           */
+int lbman_set_shape(lbman_solver* s, const lbman_shape* shape);
+/* Autotuner (no counterpart in the reference): times steps_per_trial steps
+ * of every kernel organisation x compiled tile x z-chunk candidate on the
+ * current state with CUDA events, keeps the fastest and restores the state
+ * it started from bit for bit (a temporary device copy of the fields is
+ * taken for that).  ntrials (may be NULL) receives the number of candidates
+ * timed.                                                                    */
+int lbman_autotune(lbman_solver* s, int steps_per_trial, lbman_shape* best, int* ntrials);
+
+/* Ensemble runner (no counterpart in the reference, whose solver advances one
+ * box per process).  Many independent boxes -- each with its own lbman_config
+ * (size, boundary faces, physical parameters) -- advance together: every time
+ * step is one launch per kernel covering all boxes (a persistent grid walking
+ * a box/tile work list), and lbman_ensemble_step replays steps from a CUDA
+ * graph.  All boxes share precision, advection scheme and device; the launch
+ * shape comes from boxes[0] (kernels, tile_x/y, zchunk) or from
+ * lbman_ensemble_autotune.  Each box's results are bitwise identical to
+ * running it alone through lbman_step with the same precision.              */
+typedef struct lbman_ensemble lbman_ensemble;
+int lbman_ensemble_create(const lbman_config* boxes, int nboxes, lbman_ensemble** out);
+int lbman_ensemble_destroy(lbman_ensemble* e);
+int lbman_ensemble_set_stream(lbman_ensemble* e, void* cuda_stream);
+/* Box b gets lbman_init_seeded's state with seed + b and S0 = its own
+ * equilibrium order (src/model.h:39-41).                                    */
+int lbman_ensemble_init_seeded(lbman_ensemble* e, uint64_t seed, double sigma);
+/* Before the first step only: rho, u, Q of one box; f = f_eq, F = 0.       */
+int lbman_ensemble_upload(lbman_ensemble* e, int box, const double* rho, const double* u3, const double* q5);
+int lbman_ensemble_download(lbman_ensemble* e, int box, double* rho, double* u3, double* q5, double* f15);
+int lbman_ensemble_step(lbman_ensemble* e, int nsteps);
+int lbman_ensemble_synchronize(lbman_ensemble* e);
+int lbman_ensemble_set_shape(lbman_ensemble* e, int kernels, int tile_x, int tile_y, int zchunk);
+int lbman_ensemble_get_shape(lbman_ensemble* e, lbman_shape* out);
+/* Times every kernel organisation x tile x z-chunk candidate over the whole
+ * ensemble, keeps the fastest, restores every box's state bit for bit.     */
+int lbman_ensemble_autotune(lbman_ensemble* e, int steps_per_trial, lbman_shape* best, int* ntrials);
+int lbman_ensemble_info(lbman_ensemble* e, int64_t* cells, int64_t* steps, int64_t* launches);
+
 /* Steps completed since the last upload. */
 int lbman_steps_done(lbman_solver* s, int64_t* steps);
 /* Kernel launches issued by this solver since creation (instrumentation).  */

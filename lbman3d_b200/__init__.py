@@ -11,6 +11,7 @@ from .boundary import (Anchoring, BCConfig, ChannelConfig, FullyPeriodicConfig, 
 from .device import (DeviceFields, DeviceSolver, InitializeComputeBackend, LbmSolver, QTensorSolver,
                      Simulation, make_config)
 from .fields import FluidFields, LocalGrid, QTensorFields
+from .ensemble import Ensemble, draw_boxes
 from .params import Advection, EquilibriumScalarOrder, Params, Precision
 
 __all__ = [
@@ -18,5 +19,6 @@ __all__ = [
     "Periodic", "PeriodicBC", "SimBC", "SlitConfig", "SlitNoSlipConfig", "SpecularReflection", "WallSpec",
     "from_face_tuples", "is_wall_by_face", "periodicity_by_axis", "DeviceFields", "DeviceSolver",
     "InitializeComputeBackend", "LbmSolver", "QTensorSolver", "Simulation", "make_config", "FluidFields",
-    "LocalGrid", "QTensorFields", "Advection", "EquilibriumScalarOrder", "Params", "Precision",
+    "LocalGrid", "QTensorFields", "Advection", "EquilibriumScalarOrder", "Params", "Precision", "Ensemble",
+    "draw_boxes",
 ]

@@ -42,6 +42,11 @@ class lbman_diag(C.Structure):
                 ("defect_faces", C.c_int64), ("nan_detected", C.c_int)]
 
 
+class lbman_shape(C.Structure):
+    _fields_ = [("kernels", C.c_int), ("tile_x", C.c_int), ("tile_y", C.c_int), ("zchunk", C.c_int),
+                ("threads", C.c_int), ("ms_per_step", C.c_double)]
+
+
 class LbmanError(RuntimeError):
     """A non-zero status from the C ABI (the reference throws std::runtime_error)."""
 
@@ -77,6 +82,22 @@ PROTOTYPES = [
     ("lbman_reduce", C.c_int, [C.c_void_p, C.c_int, C.POINTER(lbman_diag)]),
     ("lbman_steps_done", C.c_int, [C.c_void_p, C.POINTER(C.c_int64)]),
     ("lbman_launch_count", C.c_int, [C.c_void_p, C.POINTER(C.c_int64)]),
+    ("lbman_get_shape", C.c_int, [C.c_void_p, C.POINTER(lbman_shape)]),
+    ("lbman_set_shape", C.c_int, [C.c_void_p, C.POINTER(lbman_shape)]),
+    ("lbman_autotune", C.c_int, [C.c_void_p, C.c_int, C.POINTER(lbman_shape), C.POINTER(C.c_int)]),
+    ("lbman_ensemble_create", C.c_int, [C.POINTER(lbman_config), C.c_int, C.POINTER(C.c_void_p)]),
+    ("lbman_ensemble_destroy", C.c_int, [C.c_void_p]),
+    ("lbman_ensemble_set_stream", C.c_int, [C.c_void_p, C.c_void_p]),
+    ("lbman_ensemble_init_seeded", C.c_int, [C.c_void_p, C.c_uint64, C.c_double]),
+    ("lbman_ensemble_upload", C.c_int, [C.c_void_p, C.c_int, _DP, _DP, _DP]),
+    ("lbman_ensemble_download", C.c_int, [C.c_void_p, C.c_int, _DP, _DP, _DP, _DP]),
+    ("lbman_ensemble_step", C.c_int, [C.c_void_p, C.c_int]),
+    ("lbman_ensemble_synchronize", C.c_int, [C.c_void_p]),
+    ("lbman_ensemble_set_shape", C.c_int, [C.c_void_p, C.c_int, C.c_int, C.c_int, C.c_int]),
+    ("lbman_ensemble_get_shape", C.c_int, [C.c_void_p, C.POINTER(lbman_shape)]),
+    ("lbman_ensemble_autotune", C.c_int, [C.c_void_p, C.c_int, C.POINTER(lbman_shape), C.POINTER(C.c_int)]),
+    ("lbman_ensemble_info", C.c_int, [C.c_void_p, C.POINTER(C.c_int64), C.POINTER(C.c_int64),
+                                      C.POINTER(C.c_int64)]),
     ("lbman_flow_reduce_noalloc", C.c_int,
      [C.c_int64, C.c_int, C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p, C.POINTER(lbman_diag)]),
 ]

@@ -4,7 +4,8 @@
 
 Translation units and their flags:
   kernels_f64.cu  --fmad=false  (FP64 path, bitwise parity with the reference)
-  kernels_f32.cu  default contraction (FP32 / FP16-storage paths)
+  kernels_f32.cu  default contraction (FP32 path)
+  kernels_f16.cu  default contraction (FP16 population storage)
   api.cu          host C ABI
 Objects go to lbman3d_b200/_build/ (git-ignored).
 """
@@ -31,8 +32,11 @@ COMMON = ARCH + ["-O3", "-std=c++17", "-lineinfo", "-Xcompiler", "-fPIC", "--exp
 UNITS = {
     "kernels_f64.cu": ["--fmad=false"],
     "kernels_f32.cu": [],
+    "kernels_f16.cu": [],
     "kernels_ens.cu": [],
+    "kernels_ens_f64.cu": ["--fmad=false"],
     "api.cu": [],
+    "ens_api.cu": [],
     "noalloc.cu": [],
 }
 

@@ -58,6 +58,7 @@ struct Ops {
     decltype(&launch_defect_count_f64) defect_count;
     decltype(&launch_seeded_init_f64) seeded_init;
     decltype(&qforce_smem_f64) qforce_smem;
+    decltype(&qforce_threads_f64) qforce_threads;
     decltype(&prepare_f64) prepare;
 };
 
@@ -67,7 +68,7 @@ struct Ops {
             launch_feq_init_##SUF, launch_pop_in_##SUF, launch_pop_out_##SUF, launch_real_in_##SUF,    \
             launch_real_out_##SUF, launch_flow_reduce_##SUF, launch_energy_reduce_##SUF,               \
             launch_director_##SUF, launch_defect_count_##SUF, launch_seeded_init_##SUF,               \
-            qforce_smem_##SUF, prepare_##SUF                                                           \
+            qforce_smem_##SUF, qforce_threads_##SUF, prepare_##SUF                                     \
     }
 
 const Ops kOps[3] = {LBMAN_OPS(f64), LBMAN_OPS(f32), LBMAN_OPS(f16)};
@@ -96,6 +97,32 @@ void anchored_q(const lbman_face& f, double out[5]) {
 namespace lbman {
 // Error message for lbman_last_error() from other translation units.
 void set_last_error(const char* msg) { g_err = msg; }
+
+// params.h + BC configuration -> the kernels' SimParams.
+void build_sim_params(const lbman_config& c, SimParams& P) {
+    std::memset(&P, 0, sizeof(P));
+    P.nx = c.nx; P.ny = c.ny; P.nz = c.nz;
+    P.nxy = (int64_t)c.nx * c.ny;
+    P.V = P.nxy * c.nz;
+    P.DT = c.DT; P.kDensity = c.kDensity; P.L = c.L; P.A = c.A; P.B = c.B; P.C = c.C;
+    P.LAMBDA = c.LAMBDA; P.GAMMA = c.GAMMA; P.ALPHA = c.ALPHA; P.MU = c.MU;
+    // src/params.h:52-54
+    P.omega = 1.0 - c.DT / c.TAUF;
+    P.omega_prime = c.DT / c.TAUF;
+    P.omega_forcing = 1.0 - c.DT / 2.0 / c.TAUF;
+    P.upwind = c.advection == LBMAN_UPWIND;
+    P.moving_any = 0;
+    for (int k = 0; k < 6; ++k) {
+        P.face[k].qbc = c.face[k].qbc;
+        P.face[k].ubc = c.face[k].ubc;
+        anchored_q(c.face[k], P.face[k].anchor);
+        for (int j = 0; j < 3; ++j) P.face[k].uw[j] = c.face[k].ubc == LBMAN_U_MOVING ? c.face[k].uw[j] : 0.0;
+        P.qper[k] = c.face[k].qbc == LBMAN_Q_PERIODIC;
+        P.uper[k] = c.face[k].ubc == LBMAN_U_PERIODIC;
+        if (c.face[k].ubc == LBMAN_U_MOVING) P.moving_any = 1;
+    }
+    fill_float_phys(P);
+}
 }  // namespace lbman
 
 struct lbman_solver {
@@ -140,23 +167,52 @@ int check_launch(lbman_solver* s, cudaError_t e, const char* what) {
     return LBMAN_OK;
 }
 
-// Default z-marching shape: tile 30 x 6 (B region 32 x 8 = 256 points, one
-// per thread), z chunks sized for several waves of blocks.
-LaunchShape default_shape(const lbman_config& c, int num_sms) {
+// Compiled tile shapes of the z-marching kernels (cells per x-y plane).
+constexpr int kTiles[][2] = {{30, 6}, {32, 6}, {14, 14}, {30, 14}, {62, 6}};
+
+// z chunk giving several waves of blocks over the SMs.
+int default_zchunk(int nx, int ny, int nz, int tcx, int tcy, int num_sms) {
+    const long cols = (long)((nx + tcx - 1) / tcx) * ((ny + tcy - 1) / tcy);
+    const long target = (long)num_sms * 8;
+    long nchunks = (target + cols - 1) / cols;
+    nchunks = std::max(1L, std::min(nchunks, (long)std::max(1, nz / 8)));
+    return (int)((nz + nchunks - 1) / nchunks);
+}
+
+// Default z-marching tile before any autotuning: the widest compiled tile
+// whose last partial tile pads x by at most 10% (wide rows keep the global
+// stores of a block in full sectors); otherwise the one with the least work
+// per output cell (threads per tile cell times the x and y padding).
+LaunchShape default_shape(const lbman_config& c, int num_sms, const Ops& ops) {
     LaunchShape L;
-    L.tile.tcx = c.tile_x > 0 ? c.tile_x : 30;
-    L.tile.tcy = c.tile_y > 0 ? c.tile_y : 6;
-    const int bpts = (L.tile.tcx + 2) * (L.tile.tcy + 2);
-    L.qthreads = c.threads > 0 ? c.threads : std::min(512, ((bpts + 31) / 32) * 32);
-    if (c.zchunk > 0) {
-        L.tile.zc = c.zchunk;
+    if (c.tile_x > 0 && c.tile_y > 0) {
+        L.tile.tcx = c.tile_x;
+        L.tile.tcy = c.tile_y;
     } else {
-        const long cols = (long)((c.nx + L.tile.tcx - 1) / L.tile.tcx) * ((c.ny + L.tile.tcy - 1) / L.tile.tcy);
-        const long target = (long)num_sms * 8;
-        long nchunks = (target + cols - 1) / cols;
-        nchunks = std::max(1L, std::min(nchunks, (long)std::max(1, c.nz / 8)));
-        L.tile.zc = (int)((c.nz + nchunks - 1) / nchunks);
+        double best = 1e30;
+        int best_wide = -1;
+        L.tile.tcx = 30;
+        L.tile.tcy = 6;
+        for (const auto& t : kTiles) {
+            QTile q{t[0], t[1], 1};
+            if (ops.qforce_smem(q) == 0) continue;  // not compiled for this precision
+            const double padx = (double)((c.nx + t[0] - 1) / t[0] * t[0]) / c.nx;
+            const double pady = (double)((c.ny + t[1] - 1) / t[1] * t[1]) / c.ny;
+            const double cost = padx * pady * ops.qforce_threads(q) / (double)(t[0] * t[1]);
+            if (padx <= 1.10 && t[0] > best_wide) {
+                best_wide = t[0];
+                L.tile.tcx = t[0];
+                L.tile.tcy = t[1];
+            }
+            if (best_wide < 0 && cost < best - 1e-9) {
+                best = cost;
+                L.tile.tcx = t[0];
+                L.tile.tcy = t[1];
+            }
+        }
     }
+    L.qthreads = ops.qforce_threads(L.tile);
+    L.tile.zc = c.zchunk > 0 ? c.zchunk : default_zchunk(c.nx, c.ny, c.nz, L.tile.tcx, L.tile.tcy, num_sms);
     return L;
 }
 
@@ -207,6 +263,10 @@ int stage_out_real(lbman_solver* s, const void* src, double* host, int64_t n) {
 void* vptr(void* base, int64_t off_elems, size_t esize) { return (char*)base + off_elems * (int64_t)esize; }
 
 }  // namespace
+
+namespace lbman {
+int validate_config(const lbman_config& c) { return validate(c); }
+}  // namespace lbman
 
 extern "C" {
 
@@ -269,7 +329,10 @@ int lbman_create(const lbman_config* cfg, lbman_solver** out) {
     s->cfg = *cfg;
     s->device = cfg->device;
     s->prec = cfg->precision;
-    s->kernels = cfg->kernels == LBMAN_KERNELS_AUTO ? LBMAN_KERNELS_FUSED : cfg->kernels;
+    // Measured on B200: the split organisation (Q+force kernel, then the LBM
+    // kernel) outruns the one-kernel step for every workload and tile tried,
+    // so it is the default until lbman_autotune says otherwise.
+    s->kernels = cfg->kernels == LBMAN_KERNELS_AUTO ? LBMAN_KERNELS_SPLIT : cfg->kernels;
     s->rbytes = s->prec == LBMAN_FP64 ? 8 : 4;
     s->sbytes = s->prec == LBMAN_FP64 ? 8 : (s->prec == LBMAN_FP32 ? 4 : 2);
     auto bail = [&](int code) {
@@ -283,40 +346,23 @@ int lbman_create(const lbman_config* cfg, lbman_solver** out) {
     if (prop.major < 10) return bail(fail(LBMAN_ERR_UNSUPPORTED, "this build targets sm_100a (B200); device is sm_%d%d", prop.major, prop.minor));
     s->num_sms = prop.multiProcessorCount;
 
-    SimParams& P = s->P;
-    std::memset(&P, 0, sizeof(P));
-    P.nx = cfg->nx; P.ny = cfg->ny; P.nz = cfg->nz;
-    P.nxy = (int64_t)cfg->nx * cfg->ny;
-    P.V = P.nxy * cfg->nz;
-    P.DT = cfg->DT; P.kDensity = cfg->kDensity; P.L = cfg->L; P.A = cfg->A; P.B = cfg->B; P.C = cfg->C;
-    P.LAMBDA = cfg->LAMBDA; P.GAMMA = cfg->GAMMA; P.ALPHA = cfg->ALPHA; P.MU = cfg->MU;
-    // src/params.h:52-54
-    P.omega = 1.0 - cfg->DT / cfg->TAUF;
-    P.omega_prime = cfg->DT / cfg->TAUF;
-    P.omega_forcing = 1.0 - cfg->DT / 2.0 / cfg->TAUF;
-    P.upwind = cfg->advection == LBMAN_UPWIND;
-    P.moving_any = 0;
-    for (int k = 0; k < 6; ++k) {
-        P.face[k].qbc = cfg->face[k].qbc;
-        P.face[k].ubc = cfg->face[k].ubc;
-        anchored_q(cfg->face[k], P.face[k].anchor);
-        for (int j = 0; j < 3; ++j) P.face[k].uw[j] = cfg->face[k].ubc == LBMAN_U_MOVING ? cfg->face[k].uw[j] : 0.0;
-        P.qper[k] = cfg->face[k].qbc == LBMAN_Q_PERIODIC;
-        P.uper[k] = cfg->face[k].ubc == LBMAN_U_PERIODIC;
-        if (cfg->face[k].ubc == LBMAN_U_MOVING) P.moving_any = 1;
-    }
-
-    s->shape = default_shape(*cfg, s->num_sms);
+    build_sim_params(*cfg, s->P);
+    s->shape = default_shape(*cfg, s->num_sms, s->ops());
     const size_t smem = s->ops().qforce_smem(s->shape.tile);
+    if (smem == 0)
+        return bail(fail(LBMAN_ERR_ARG, "tile %dx%d is not compiled for this precision (compiled: 30x6, 32x6, "
+                                        "14x14, and for FP32/FP16 also 30x14, 62x6)",
+                         s->shape.tile.tcx, s->shape.tile.tcy));
     if (smem > (size_t)prop.sharedMemPerBlockOptin)
         return bail(fail(LBMAN_ERR_ARG, "tile %dx%d needs %zu B of shared memory (max %zu)", s->shape.tile.tcx,
                          s->shape.tile.tcy, smem, (size_t)prop.sharedMemPerBlockOptin));
-    if (s->shape.qthreads % 32 || s->shape.qthreads > 512 || s->shape.qthreads < 32)
-        return bail(fail(LBMAN_ERR_ARG, "threads must be a multiple of 32 in [32, 512]"));
+    if (cfg->threads > 0 && cfg->threads != s->shape.qthreads)
+        return bail(fail(LBMAN_ERR_ARG, "tile %dx%d runs %d threads per block", s->shape.tile.tcx,
+                         s->shape.tile.tcy, s->shape.qthreads));
     if (cudaError_t e = s->ops().prepare(prop.sharedMemPerBlockOptin))
         return bail(fail(LBMAN_ERR_CUDA, "cudaFuncSetAttribute: %s", cudaGetErrorString(e)));
 
-    const int64_t V = P.V;
+    const int64_t V = s->P.V;
     auto alloc = [&](void** p, size_t bytes) -> int {
         cudaError_t e = cudaMalloc(p, bytes);
         if (e != cudaSuccess) return fail(LBMAN_ERR_NOMEM, "cudaMalloc(%zu) failed: %s", bytes, cudaGetErrorString(e));
@@ -539,6 +585,110 @@ int lbman_reduce(lbman_solver* s, int flags, lbman_diag* out) {
     if (flags & LBMAN_DIAG_ENERGY) out->free_energy = r[8];
     if (defects) out->defect_faces = (int64_t)std::llround(r[9]);
     if (out->nan_detected) return fail(LBMAN_ERR_DIVERGED, "NaN in the global mass or momentum");
+    return LBMAN_OK;
+}
+
+int lbman_get_shape(lbman_solver* s, lbman_shape* out) {
+    if (!s || !out) return fail(LBMAN_ERR_ARG, "null argument");
+    out->kernels = s->kernels;
+    out->tile_x = s->shape.tile.tcx;
+    out->tile_y = s->shape.tile.tcy;
+    out->zchunk = s->shape.tile.zc;
+    out->threads = s->shape.qthreads;
+    out->ms_per_step = 0.0;
+    return LBMAN_OK;
+}
+
+int lbman_set_shape(lbman_solver* s, const lbman_shape* sh) {
+    if (!s || !sh) return fail(LBMAN_ERR_ARG, "null argument");
+    if (sh->kernels != LBMAN_KERNELS_SPLIT && sh->kernels != LBMAN_KERNELS_FUSED)
+        return fail(LBMAN_ERR_ARG, "kernels must be LBMAN_KERNELS_SPLIT or LBMAN_KERNELS_FUSED");
+    QTile t{sh->tile_x, sh->tile_y, sh->zchunk};
+    if (sh->zchunk < 1) return fail(LBMAN_ERR_ARG, "zchunk must be >= 1");
+    if (s->ops().qforce_smem(t) == 0)
+        return fail(LBMAN_ERR_ARG, "tile %dx%d is not compiled for this precision", sh->tile_x, sh->tile_y);
+    s->kernels = sh->kernels;
+    s->shape.tile = t;
+    s->shape.qthreads = s->ops().qforce_threads(t);
+    return LBMAN_OK;
+}
+
+int lbman_autotune(lbman_solver* s, int steps_per_trial, lbman_shape* best, int* ntrials) {
+    if (!s || !best) return fail(LBMAN_ERR_ARG, "null argument");
+    if (!s->uploaded) return fail(LBMAN_ERR_STATE, "autotune needs an uploaded state");
+    if (steps_per_trial < 1) return fail(LBMAN_ERR_ARG, "steps_per_trial must be >= 1");
+    LB_TRY(set_device(s));
+    const int64_t V = s->P.V;
+    // Snapshot of the state the trials will advance.
+    const size_t fb = 15 * V * s->sbytes, qb = 5 * V * s->rbytes, ub = 3 * V * s->rbytes, rb = V * s->rbytes;
+    char* snap = nullptr;
+    LB_CUDA(cudaMalloc(&snap, fb + qb + ub + rb + ub));
+    const int fc = s->fcur, qc = s->qcur, uc = s->ucur;
+    const bool fpost = s->f_post;
+    const int64_t steps0 = s->steps;
+    auto copy_state = [&](bool save) -> cudaError_t {
+        void* dst[5] = {snap, snap + fb, snap + fb + qb, snap + fb + qb + ub, snap + fb + qb + ub + rb};
+        void* src[5] = {s->f[fc], s->q[qc], s->u[uc], s->rho, s->F};
+        const size_t n[5] = {fb, qb, ub, rb, ub};
+        for (int k = 0; k < 5; ++k) {
+            cudaError_t e = save ? cudaMemcpyAsync(dst[k], src[k], n[k], cudaMemcpyDeviceToDevice, s->stream)
+                                 : cudaMemcpyAsync(src[k], dst[k], n[k], cudaMemcpyDeviceToDevice, s->stream);
+            if (e != cudaSuccess) return e;
+        }
+        return cudaSuccess;
+    };
+    cudaEvent_t e0 = nullptr, e1 = nullptr;
+    int status = LBMAN_OK, count = 0;
+    lbman_shape orig, cur{}, win{};
+    lbman_get_shape(s, &orig);
+    win = orig;
+    win.ms_per_step = 1e30;
+    if (copy_state(true) != cudaSuccess || cudaEventCreate(&e0) != cudaSuccess || cudaEventCreate(&e1) != cudaSuccess) {
+        status = fail(LBMAN_ERR_CUDA, "autotune set-up failed");
+    } else {
+        for (int k : {LBMAN_KERNELS_SPLIT, LBMAN_KERNELS_FUSED}) {
+            for (const auto& t : kTiles) {
+                QTile q{t[0], t[1], 1};
+                if (s->ops().qforce_smem(q) == 0) continue;
+                const int z0 = default_zchunk(s->P.nx, s->P.ny, s->P.nz, t[0], t[1], s->num_sms);
+                int zs[3] = {z0, std::max(4, z0 / 2), std::min(s->P.nz, 2 * z0)};
+                for (int zi = 0; zi < 3 && status == LBMAN_OK; ++zi) {
+                    if (zi > 0 && (zs[zi] == z0 || (zi == 2 && zs[2] == zs[1]))) continue;
+                    cur = {k, t[0], t[1], zs[zi], 0, 0.0};
+                    if (lbman_set_shape(s, &cur) != LBMAN_OK) continue;
+                    if ((status = one_step(s, false)) != LBMAN_OK) break;
+                    cudaEventRecord(e0, s->stream);
+                    for (int n = 0; n < steps_per_trial && status == LBMAN_OK; ++n) status = one_step(s, false);
+                    cudaEventRecord(e1, s->stream);
+                    if (status != LBMAN_OK) break;
+                    if (cudaEventSynchronize(e1) != cudaSuccess) {
+                        status = fail(LBMAN_ERR_CUDA, "autotune trial failed");
+                        break;
+                    }
+                    float ms = 0.f;
+                    cudaEventElapsedTime(&ms, e0, e1);
+                    cur.ms_per_step = ms / steps_per_trial;
+                    ++count;
+                    if (cur.ms_per_step < win.ms_per_step) win = cur;
+                }
+            }
+        }
+    }
+    // Restore the state and the indices it lived in, then adopt the winner.
+    if (copy_state(false) != cudaSuccess && status == LBMAN_OK) status = fail(LBMAN_ERR_CUDA, "state restore failed");
+    cudaStreamSynchronize(s->stream);
+    s->fcur = fc; s->qcur = qc; s->ucur = uc; s->f_post = fpost; s->steps = steps0;
+    if (e0) cudaEventDestroy(e0);
+    if (e1) cudaEventDestroy(e1);
+    cudaFree(snap);
+    if (status != LBMAN_OK) {
+        lbman_set_shape(s, &orig);
+        return status;
+    }
+    lbman_set_shape(s, &win);
+    lbman_get_shape(s, best);
+    best->ms_per_step = win.ms_per_step;
+    if (ntrials) *ntrials = count;
     return LBMAN_OK;
 }
 

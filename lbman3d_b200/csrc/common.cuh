@@ -21,6 +21,16 @@ struct Face {
     double uw[3];
 };
 
+// Physical constants in compute precision R (the FP32 copy is rounded once
+// on the host, so kernels do no double-to-float conversions).
+template <class R>
+struct Phys {
+    R DT, kDensity, L, A, B, C, LAMBDA, GAMMA, ALPHA, MU;
+    R omega, omega_prime, omega_forcing;
+    R anchor[6][5];
+    R uw[6][3];
+};
+
 // params.h + SimBC at run time.  Passed by value to every kernel.
 struct SimParams {
     int nx, ny, nz;
@@ -31,7 +41,39 @@ struct SimParams {
     Face face[6];          // XLo, XHi, YLo, YHi, ZLo, ZHi
     int qper[6], uper[6];  // face tag is Periodic (Q / velocity)
     int moving_any;        // some face is a MovingWall
+    Phys<double> pd;       // the constants above, per compute precision; kernels
+    Phys<float> pf;        // read them in place from the parameter space
 };
+
+// Constants of precision R, referenced inside the kernel's (grid-constant)
+// parameter struct, so dynamic indexing needs no local copy.
+template <class R>
+__host__ __device__ inline const Phys<R>& phys_ref(const SimParams& P);
+template <>
+__host__ __device__ inline const Phys<float>& phys_ref<float>(const SimParams& P) {
+    return P.pf;
+}
+template <>
+__host__ __device__ inline const Phys<double>& phys_ref<double>(const SimParams& P) {
+    return P.pd;
+}
+
+// Fills P.pd / P.pf from the double fields (host side, once per solver).
+template <class R>
+inline void fill_phys(const SimParams& P, Phys<R>& k) {
+    k.DT = (R)P.DT; k.kDensity = (R)P.kDensity; k.L = (R)P.L; k.A = (R)P.A;
+    k.B = (R)P.B; k.C = (R)P.C; k.LAMBDA = (R)P.LAMBDA; k.GAMMA = (R)P.GAMMA;
+    k.ALPHA = (R)P.ALPHA; k.MU = (R)P.MU; k.omega = (R)P.omega;
+    k.omega_prime = (R)P.omega_prime; k.omega_forcing = (R)P.omega_forcing;
+    for (int f = 0; f < 6; ++f) {
+        for (int c = 0; c < 5; ++c) k.anchor[f][c] = (R)P.face[f].anchor[c];
+        for (int c = 0; c < 3; ++c) k.uw[f][c] = (R)P.face[f].uw[c];
+    }
+}
+inline void fill_float_phys(SimParams& P) {
+    fill_phys<double>(P, P.pd);
+    fill_phys<float>(P, P.pf);
+}
 
 // z-marching tile of the Q+force kernel (runtime shape, chosen by the autotuner).
 struct QTile {

@@ -17,45 +17,56 @@
 
 namespace lbman {
 
-template <class R, class S, bool DEV, bool UPWIND, bool FIRST>
-__global__ void __launch_bounds__(512) fused_kernel(SimParams P, QTile T, const R* __restrict__ qin,
-                                                    const R* __restrict__ uin, R* __restrict__ qout,
-                                                    R* __restrict__ uout, const S* __restrict__ fin,
-                                                    S* __restrict__ fout, R* __restrict__ rho_buf,
-                                                    R* __restrict__ Fout, int write_rho_all) {
+// Consumer of the fused organisation: store Q_new (and F on request), then
+// gather, collide and store this cell's populations, velocity and density.
+template <class R, class S, bool DEV>
+struct CollideCell {
+    const SimParams& P;
+    const Phys<R>& K;
+    int first;
+    R* __restrict__ qout;
+    R* __restrict__ uout;
+    const S* __restrict__ fin;
+    S* __restrict__ fout;
+    R* __restrict__ rho_buf;
+    R* __restrict__ Fout;
+    int write_rho_all;
+    __device__ __forceinline__ void operator()(int64_t cell, int x, int y, int z, const R qn[5], const R F[3],
+                                               const R*) const {
+        const int64_t V = P.V;
+#pragma unroll
+        for (int k = 0; k < 5; ++k) qout[k * V + cell] = qn[k];
+        if (Fout) {
+            Fout[cell] = F[0];
+            Fout[V + cell] = F[1];
+            Fout[2 * V + cell] = F[2];
+        }
+        const bool mv = P.moving_any && touches_moving(P, x, y, z);
+        R f[15];
+        load_pre<R, S>(P, K, first != 0, fin, cell, CellPos{x, y, z}, (mv && !first) ? rho_buf[cell] : R(0), f);
+        R rho, ux, uy, uz;
+        collide<R, DEV>(K, f, F[0], F[1], F[2], rho, ux, uy, uz);
+#pragma unroll
+        for (int j = 0; j < 15; ++j) Store<S>::st(fout + j * V + cell, f[j]);
+        uout[cell] = ux;
+        uout[V + cell] = uy;
+        uout[2 * V + cell] = uz;
+        if (write_rho_all || mv) rho_buf[cell] = rho;
+    }
+};
+
+template <class TL, class R, class S, bool DEV, bool UPWIND>
+__global__ void __launch_bounds__(TL::NT) fused_kernel(const __grid_constant__ SimParams P, int zc_len, int first,
+                                                       const R* __restrict__ qin, const R* __restrict__ uin,
+                                                       R* __restrict__ qout, R* __restrict__ uout,
+                                                       const S* __restrict__ fin, S* __restrict__ fout,
+                                                       R* __restrict__ rho_buf, R* __restrict__ Fout,
+                                                       int write_rho_all) {
     extern __shared__ __align__(16) unsigned char smem_raw[];
-    R* QU = reinterpret_cast<R*>(smem_raw);
-    R* Bs = QU + qf_qu_elems<R>(T);
-    const int64_t V = P.V;
-    qf_march<R, UPWIND>(P, T, qin, uin, QU, Bs, [&](int x0, int y0, int z0, int zc) {
-        qf_force_plane<R>(P, T, x0, y0, z0, zc, QU, Bs,
-                          [&](int64_t cell, int x, int y, int z, const R qn[5], const R F[3], const R*) {
-#pragma unroll
-                              for (int k = 0; k < 5; ++k) qout[k * V + cell] = qn[k];
-                              if (Fout) {
-                                  Fout[cell] = F[0];
-                                  Fout[V + cell] = F[1];
-                                  Fout[2 * V + cell] = F[2];
-                              }
-                              const bool mv = P.moving_any && touches_moving(P, x, y, z);
-                              R f[15];
-                              if (FIRST) {
-#pragma unroll
-                                  for (int j = 0; j < 15; ++j) f[j] = Store<S>::ld(fin + j * V + cell);
-                              } else {
-                                  CellPos q{x, y, z};
-                                  gather<R, S>(P, fin, cell, q, mv ? rho_buf[cell] : R(0), f);
-                              }
-                              R rho, ux, uy, uz;
-                              collide<R, DEV>(P, f, F[0], F[1], F[2], rho, ux, uy, uz);
-#pragma unroll
-                              for (int j = 0; j < 15; ++j) Store<S>::st(fout + j * V + cell, f[j]);
-                              uout[cell] = ux;
-                              uout[V + cell] = uy;
-                              uout[2 * V + cell] = uz;
-                              if (write_rho_all || mv) rho_buf[cell] = rho;
-                          });
-    });
+    qf_march<TL, R, UPWIND>(
+        P, zc_len, qin, uin, reinterpret_cast<R*>(smem_raw),
+        CollideCell<R, S, DEV>{P, phys_ref<R>(P), first, qout, uout, fin, fout, rho_buf, Fout, write_rho_all},
+        blockIdx.x, blockIdx.y, blockIdx.z);
 }
 
 }  // namespace lbman

@@ -7,49 +7,96 @@
 #include "launch.h"
 #include "reduce.cuh"
 
+#include <utility>
+
 namespace lbman {
 namespace impl {
 
 inline unsigned blocks_for(int64_t n, int threads) { return (unsigned)((n + threads - 1) / threads); }
 
-inline dim3 qgrid(const SimParams& P, const QTile& T) {
-    return dim3((unsigned)((P.nx + T.tcx - 1) / T.tcx), (unsigned)((P.ny + T.tcy - 1) / T.tcy),
-                (unsigned)((P.nz + T.zc - 1) / T.zc));
+inline dim3 qgrid(const SimParams& P, int tcx, int tcy, int zc) {
+    return dim3((unsigned)((P.nx + tcx - 1) / tcx), (unsigned)((P.ny + tcy - 1) / tcy),
+                (unsigned)((P.nz + zc - 1) / zc));
+}
+
+constexpr size_t kMaxSmem = 227 * 1024;
+
+// Calls f(Tile<...>{}) for the compiled tile shape (tcx, tcy); tiles whose
+// staging does not fit in one block's shared memory for this precision are
+// not instantiated.  Returns cudaErrorInvalidValue for any other shape.
+template <class R, class F>
+cudaError_t with_tile(int tcx, int tcy, F&& f) {
+#define LBMAN_TILE(X, Y)                                                   \
+    if (tcx == X && tcy == Y) {                                            \
+        if constexpr (Tile<X, Y>::template smem_bytes<R>() <= kMaxSmem)    \
+            return f(Tile<X, Y>{});                                        \
+        else                                                               \
+            return cudaErrorInvalidValue;                                  \
+    }
+    LBMAN_TILE(30, 6)
+    LBMAN_TILE(32, 6)
+    LBMAN_TILE(14, 14)
+    LBMAN_TILE(30, 14)
+    LBMAN_TILE(62, 6)
+#undef LBMAN_TILE
+    return cudaErrorInvalidValue;
 }
 
 template <class R>
 size_t qforce_smem(const QTile& T) {
-    return qforce_smem_bytes(T, sizeof(R));
+    size_t b = 0;
+    with_tile<R>(T.tcx, T.tcy, [&](auto tl) {
+        b = decltype(tl)::template smem_bytes<R>();
+        return cudaSuccess;
+    });
+    return b;
+}
+
+template <class R>
+int qforce_threads(const QTile& T) {
+    int n = 0;
+    with_tile<R>(T.tcx, T.tcy, [&](auto tl) {
+        n = decltype(tl)::NT;
+        return cudaSuccess;
+    });
+    return n;
 }
 
 template <class R>
 cudaError_t qforce(const SimParams& P, const LaunchShape& S, const void* qin, const void* uin, void* qout,
                    void* Fout, cudaStream_t st) {
-    const size_t smem = qforce_smem<R>(S.tile);
-    if (P.upwind)
-        qforce_kernel<R, true><<<qgrid(P, S.tile), S.qthreads, smem, st>>>(
-            P, S.tile, (const R*)qin, (const R*)uin, (R*)qout, (R*)Fout);
-    else
-        qforce_kernel<R, false><<<qgrid(P, S.tile), S.qthreads, smem, st>>>(
-            P, S.tile, (const R*)qin, (const R*)uin, (R*)qout, (R*)Fout);
-    return cudaGetLastError();
+    return with_tile<R>(S.tile.tcx, S.tile.tcy, [&](auto tl) {
+        using TL = decltype(tl);
+        const dim3 g = qgrid(P, TL::TCX, TL::TCY, S.tile.zc);
+        const size_t smem = TL::template smem_bytes<R>();
+        if (P.upwind)
+            qforce_kernel<TL, R, true><<<g, TL::NT, smem, st>>>(P, S.tile.zc, (const R*)qin, (const R*)uin,
+                                                               (R*)qout, (R*)Fout);
+        else
+            qforce_kernel<TL, R, false><<<g, TL::NT, smem, st>>>(P, S.tile.zc, (const R*)qin, (const R*)uin,
+                                                                (R*)qout, (R*)Fout);
+        return cudaGetLastError();
+    });
 }
 
 template <class R, class S, bool DEV>
 cudaError_t fused(const SimParams& P, const LaunchShape& L, bool first, const void* qin, const void* uin,
                   void* qout, void* uout, const void* fin, void* fout, void* rho, void* Fout, bool wr,
                   cudaStream_t st) {
-    const size_t smem = qforce_smem<R>(L.tile);
-    const dim3 g = qgrid(P, L.tile);
-#define LBMAN_FUSED(UP, FI)                                                                           \
-    fused_kernel<R, S, DEV, UP, FI><<<g, L.qthreads, smem, st>>>(P, L.tile, (const R*)qin,            \
-                                                                 (const R*)uin, (R*)qout, (R*)uout,   \
-                                                                 (const S*)fin, (S*)fout, (R*)rho,    \
-                                                                 (R*)Fout, wr ? 1 : 0)
-    if (P.upwind) { if (first) LBMAN_FUSED(true, true); else LBMAN_FUSED(true, false); }
-    else { if (first) LBMAN_FUSED(false, true); else LBMAN_FUSED(false, false); }
-#undef LBMAN_FUSED
-    return cudaGetLastError();
+    return with_tile<R>(L.tile.tcx, L.tile.tcy, [&](auto tl) {
+        using TL = decltype(tl);
+        const dim3 g = qgrid(P, TL::TCX, TL::TCY, L.tile.zc);
+        const size_t smem = TL::template smem_bytes<R>();
+        auto launch = [&](auto kern) {
+            kern<<<g, TL::NT, smem, st>>>(P, L.tile.zc, first ? 1 : 0, (const R*)qin, (const R*)uin, (R*)qout,
+                                          (R*)uout, (const S*)fin, (S*)fout, (R*)rho, (R*)Fout, wr ? 1 : 0);
+        };
+        if (P.upwind)
+            launch(fused_kernel<TL, R, S, DEV, true>);
+        else
+            launch(fused_kernel<TL, R, S, DEV, false>);
+        return cudaGetLastError();
+    });
 }
 
 template <class R, class S, bool DEV>
@@ -57,12 +104,8 @@ cudaError_t lbm(const SimParams& P, bool first, bool wr, const void* fin, void* 
                 void* rho, void* uout, cudaStream_t st) {
     const FastDiv dnx = make_fastdiv((uint32_t)P.nx), dnxy = make_fastdiv((uint32_t)P.nxy);
     const unsigned nb = blocks_for(P.V, 256);
-    if (first)
-        lbm_kernel<R, S, DEV, true><<<nb, 256, 0, st>>>(P, dnx, dnxy, (const S*)fin, (S*)fout, (const R*)F,
-                                                        (R*)rho, (R*)uout, wr ? 1 : 0);
-    else
-        lbm_kernel<R, S, DEV, false><<<nb, 256, 0, st>>>(P, dnx, dnxy, (const S*)fin, (S*)fout, (const R*)F,
-                                                         (R*)rho, (R*)uout, wr ? 1 : 0);
+    lbm_kernel<R, S, DEV><<<nb, 256, 0, st>>>(P, dnx, dnxy, first ? 1 : 0, (const S*)fin, (S*)fout,
+                                              (const R*)F, (R*)rho, (R*)uout, wr ? 1 : 0);
     return cudaGetLastError();
 }
 
@@ -157,15 +200,19 @@ template <class R, class S, bool DEV>
 cudaError_t prepare(size_t max_smem) {
     const int b = (int)max_smem;
     cudaError_t e = cudaSuccess;
-#define LBMAN_ATTR(K) \
-    if (e == cudaSuccess) e = cudaFuncSetAttribute(K, cudaFuncAttributeMaxDynamicSharedMemorySize, b)
-    LBMAN_ATTR((qforce_kernel<R, true>));
-    LBMAN_ATTR((qforce_kernel<R, false>));
-    LBMAN_ATTR((fused_kernel<R, S, DEV, true, true>));
-    LBMAN_ATTR((fused_kernel<R, S, DEV, true, false>));
-    LBMAN_ATTR((fused_kernel<R, S, DEV, false, true>));
-    LBMAN_ATTR((fused_kernel<R, S, DEV, false, false>));
-#undef LBMAN_ATTR
+    auto attr = [&](auto kern) {
+        if (e == cudaSuccess) e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, b);
+    };
+    for (auto [x, y] : {std::pair<int, int>{30, 6}, {32, 6}, {14, 14}, {30, 14}, {62, 6}}) {
+        with_tile<R>(x, y, [&](auto tl) {
+            using TL = decltype(tl);
+            attr(qforce_kernel<TL, R, true>);
+            attr(qforce_kernel<TL, R, false>);
+            attr(fused_kernel<TL, R, S, DEV, true>);
+            attr(fused_kernel<TL, R, S, DEV, false>);
+            return cudaSuccess;
+        });
+    }
     return e;
 }
 
@@ -233,5 +280,6 @@ cudaError_t prepare(size_t max_smem) {
         return impl::seeded_init<R>(P, seed, S0, sigma, rho, u, q, F, st);                              \
     }                                                                                                   \
     size_t qforce_smem_##SUF(const QTile& T) { return impl::qforce_smem<R>(T); }                       \
+    int qforce_threads_##SUF(const QTile& T) { return impl::qforce_threads<R>(T); }                    \
     cudaError_t prepare_##SUF(size_t max_smem) { return impl::prepare<R, S, DEV>(max_smem); }           \
     }

@@ -48,6 +48,7 @@ struct LaunchShape {
     cudaError_t launch_seeded_init_##SUF(const SimParams& P, uint64_t seed, double S0, double sigma,    \
                                          void* rho, void* u, void* q, void* F, cudaStream_t st);       \
     size_t qforce_smem_##SUF(const QTile& T);                                                          \
+    int qforce_threads_##SUF(const QTile& T);                                                          \
     cudaError_t prepare_##SUF(size_t max_smem);
 
 LBMAN_DECLARE_LAUNCHERS(f64)

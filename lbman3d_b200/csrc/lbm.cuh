@@ -74,39 +74,42 @@ __device__ __forceinline__ bool touches_moving(const SimParams& P, int x, int y,
 // Gather the 15 pre-collision populations of cell c from the post-collision
 // buffer fin (see the rule above).
 template <class R, class S>
-__device__ __forceinline__ void gather(const SimParams& P, const S* __restrict__ fin, int64_t c,
-                                       CellPos q, R rho_prev, R f[15]) {
+__device__ __forceinline__ void gather(const SimParams& P, const Phys<R>& K, const S* __restrict__ fin,
+                                       int64_t c, CellPos q, R rho_prev, R f[15]) {
     const int64_t V = P.V;
     const int nx = P.nx, ny = P.ny, nz = P.nz;
-    const bool interior = q.x > 0 && q.x < nx - 1 && q.y > 0 && q.y < ny - 1 && q.z > 0 && q.z < nz - 1;
-    if (interior) {
-#pragma unroll
-        for (int j = 0; j < 15; ++j)
-            f[j] = Store<S>::ld(fin + j * V + c - (ex_(j) + (int64_t)ey_(j) * nx + (int64_t)ez_(j) * P.nxy));
-        return;
-    }
+    // Offsets of the source cell c - e along each axis for e = +1 / -1, with
+    // the periodic wrap folded in, and whether that source lies beyond a wall
+    // (velocity tags are periodic on both faces of an axis or on neither).
+    const bool lox = q.x == 0, hix = q.x == nx - 1, loy = q.y == 0, hiy = q.y == ny - 1;
+    const bool loz = q.z == 0, hiz = q.z == nz - 1;
+    const int64_t ox_m = lox ? (int64_t)(nx - 1) : -1, ox_p = hix ? (int64_t)(1 - nx) : 1;
+    const int64_t oy_m = loy ? (int64_t)(ny - 1) * nx : -(int64_t)nx;
+    const int64_t oy_p = hiy ? -(int64_t)(ny - 1) * nx : (int64_t)nx;
+    const int64_t oz_m = loz ? (int64_t)(nz - 1) * P.nxy : -P.nxy;
+    const int64_t oz_p = hiz ? -(int64_t)(nz - 1) * P.nxy : P.nxy;
+    const bool wx = !P.uper[0], wy = !P.uper[2], wz = !P.uper[4];
 #pragma unroll
     for (int j = 0; j < 15; ++j) {
-        int sx = q.x - ex_(j), sy = q.y - ey_(j), sz = q.z - ez_(j);
-        int cross = 0, fxs = 0, fys = 0, fzs = 0;
-        if (sx < 0) { if (P.uper[0]) sx += nx; else { cross |= 1; fxs = 0; } }
-        else if (sx >= nx) { if (P.uper[1]) sx -= nx; else { cross |= 1; fxs = 1; } }
-        if (sy < 0) { if (P.uper[2]) sy += ny; else { cross |= 2; fys = 2; } }
-        else if (sy >= ny) { if (P.uper[3]) sy -= ny; else { cross |= 2; fys = 3; } }
-        if (sz < 0) { if (P.uper[4]) sz += nz; else { cross |= 4; fzs = 4; } }
-        else if (sz >= nz) { if (P.uper[5]) sz -= nz; else { cross |= 4; fzs = 5; } }
-        if (!cross) {
-            f[j] = Store<S>::ld(fin + j * V + (int64_t)sz * P.nxy + (int64_t)sy * nx + sx);
+        // source = c - e_j: e = +1 looks at the -1 neighbour
+        const int64_t off = (ex_(j) > 0 ? ox_m : ex_(j) < 0 ? ox_p : 0) +
+                            (ey_(j) > 0 ? oy_m : ey_(j) < 0 ? oy_p : 0) + (ez_(j) > 0 ? oz_m : ez_(j) < 0 ? oz_p : 0);
+        const bool cx = wx && ((ex_(j) > 0 && lox) || (ex_(j) < 0 && hix));
+        const bool cy = wy && ((ey_(j) > 0 && loy) || (ey_(j) < 0 && hiy));
+        const bool cz = wz && ((ez_(j) > 0 && loz) || (ez_(j) < 0 && hiz));
+        if (!(cx || cy || cz)) {
+            f[j] = Store<S>::ld(fin + j * V + c + off);
             continue;
         }
+        const int cross = (cx ? 1 : 0) | (cy ? 2 : 0) | (cz ? 4 : 0);
+        const int fxs = ex_(j) > 0 ? 0 : 1, fys = ey_(j) > 0 ? 2 : 3, fzs = ez_(j) > 0 ? 4 : 5;
         int bi = -1, bf = 0;
         if (cross & 1) { const int i = P.face[fxs].ubc == U_SPECULAR ? spec_(0, j) : opp_(j); if (i >= bi) { bi = i; bf = fxs; } }
         if (cross & 2) { const int i = P.face[fys].ubc == U_SPECULAR ? spec_(1, j) : opp_(j); if (i >= bi) { bi = i; bf = fys; } }
         if (cross & 4) { const int i = P.face[fzs].ubc == U_SPECULAR ? spec_(2, j) : opp_(j); if (i >= bi) { bi = i; bf = fzs; } }
         R v = Store<S>::ld(fin + (int64_t)bi * V + c);
         if (P.face[bf].ubc == U_MOVING) {
-            const R dot = R(ex_(j)) * R(P.face[bf].uw[0]) + R(ey_(j)) * R(P.face[bf].uw[1]) +
-                          R(ez_(j)) * R(P.face[bf].uw[2]);
+            const R dot = R(ex_(j)) * K.uw[bf][0] + R(ey_(j)) * K.uw[bf][1] + R(ez_(j)) * K.uw[bf][2];
             v = v + R(6.0) * rho_prev * w_<R>(j) * dot;
         }
         f[j] = v;
@@ -116,9 +119,9 @@ __device__ __forceinline__ void gather(const SimParams& P, const S* __restrict__
 // Moments, equilibrium, Guo forcing and BGK relaxation of one cell
 // (src/physics_helpers.h:69-129); f is overwritten with f*.
 template <class R, bool DEV>
-__device__ __forceinline__ void collide(const SimParams& P, R f[15], R Fx, R Fy, R Fz, R& rho, R& ux,
+__device__ __forceinline__ void collide(const Phys<R>& K, R f[15], R Fx, R Fy, R Fz, R& rho, R& ux,
                                         R& uy, R& uz) {
-    const R DT = R(P.DT);
+    const R DT = K.DT;
     R s = f[0];
 #pragma unroll
     for (int j = 1; j < 15; ++j) s = s + f[j];
@@ -130,14 +133,21 @@ __device__ __forceinline__ void collide(const SimParams& P, R f[15], R Fx, R Fy,
         if (ey_(j)) { const R t = sgn_term(ey_(j), f[j]); jy = hy ? jy + t : t; hy = true; }
         if (ez_(j)) { const R t = sgn_term(ez_(j), f[j]); jz = hz ? jz + t : t; hz = true; }
     }
-    const R rho0 = R(P.kDensity);
+    const R rho0 = K.kDensity;
     rho = DEV ? rho0 + s : s;  // DEV: s is the density deviation
-    ux = (jx + R(0.5) * Fx * DT) / rho;
-    uy = (jy + R(0.5) * Fy * DT) / rho;
-    uz = (jz + R(0.5) * Fz * DT) / rho;
+    if constexpr (sizeof(R) == 8) {  // the reference's divisions, for bitwise FP64 parity
+        ux = (jx + R(0.5) * Fx * DT) / rho;
+        uy = (jy + R(0.5) * Fy * DT) / rho;
+        uz = (jz + R(0.5) * Fz * DT) / rho;
+    } else {
+        const R inv = R(1) / rho;
+        ux = (jx + R(0.5) * Fx * DT) * inv;
+        uy = (jy + R(0.5) * Fy * DT) * inv;
+        uz = (jz + R(0.5) * Fz * DT) * inv;
+    }
     const R uF = ux * Fx + uy * Fy + uz * Fz;
     const R u2 = ux * ux + uy * uy + uz * uz;
-    const R om = R(P.omega), omp = R(P.omega_prime), omf = R(P.omega_forcing);
+    const R om = K.omega, omp = K.omega_prime, omf = K.omega_forcing;
 #pragma unroll
     for (int j = 0; j < 15; ++j) {
         const R w = w_<R>(j);
@@ -151,15 +161,29 @@ __device__ __forceinline__ void collide(const SimParams& P, R f[15], R Fx, R Fy,
     }
 }
 
-// One LBM step.  FIRST: fin holds pre-collision populations (just uploaded).
-template <class R, class S, bool DEV, bool FIRST>
-__global__ void __launch_bounds__(256) lbm_kernel(SimParams P, FastDiv dnx, FastDiv dnxy,
+// Pre-collision populations of cell c: read in place on the first step after
+// an upload, gathered from the neighbours' f* otherwise.
+template <class R, class S>
+__device__ __forceinline__ void load_pre(const SimParams& P, const Phys<R>& K, bool first,
+                                         const S* __restrict__ fin, int64_t c, CellPos q, R rho_prev, R f[15]) {
+    if (first) {
+#pragma unroll
+        for (int j = 0; j < 15; ++j) f[j] = Store<S>::ld(fin + j * P.V + c);
+    } else {
+        gather<R, S>(P, K, fin, c, q, rho_prev, f);
+    }
+}
+
+// One LBM step.  first: fin holds pre-collision populations (just uploaded).
+template <class R, class S, bool DEV>
+__global__ void __launch_bounds__(256) lbm_kernel(const __grid_constant__ SimParams P, FastDiv dnx, FastDiv dnxy, int first,
                                                   const S* __restrict__ fin, S* __restrict__ fout,
                                                   const R* __restrict__ F, R* __restrict__ rho_buf,
                                                   R* __restrict__ uout, int write_rho_all) {
     const int64_t c = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
     if (c >= P.V) return;
     const int64_t V = P.V;
+    const Phys<R>& K = phys_ref<R>(P);
     CellPos q;
     q.z = (int)fdiv((uint32_t)c, dnxy);
     const uint32_t r = (uint32_t)(c - (int64_t)q.z * P.nxy);
@@ -167,15 +191,9 @@ __global__ void __launch_bounds__(256) lbm_kernel(SimParams P, FastDiv dnx, Fast
     q.x = (int)(r - (uint32_t)q.y * (uint32_t)P.nx);
     const bool mv = P.moving_any && touches_moving(P, q.x, q.y, q.z);
     R f[15];
-    if (FIRST) {
-#pragma unroll
-        for (int j = 0; j < 15; ++j) f[j] = Store<S>::ld(fin + j * V + c);
-    } else {
-        const R rp = mv ? rho_buf[c] : R(0);
-        gather<R, S>(P, fin, c, q, rp, f);
-    }
+    load_pre<R, S>(P, K, first != 0, fin, c, q, (mv && !first) ? rho_buf[c] : R(0), f);
     R rho, ux, uy, uz;
-    collide<R, DEV>(P, f, F[c], F[V + c], F[2 * V + c], rho, ux, uy, uz);
+    collide<R, DEV>(K, f, F[c], F[V + c], F[2 * V + c], rho, ux, uy, uz);
 #pragma unroll
     for (int j = 0; j < 15; ++j) Store<S>::st(fout + j * V + c, f[j]);
     uout[c] = ux;
@@ -187,7 +205,7 @@ __global__ void __launch_bounds__(256) lbm_kernel(SimParams P, FastDiv dnx, Fast
 // Pre-collision populations from the stored post-collision ones (for a
 // download of f): the gather alone.
 template <class R, class S>
-__global__ void __launch_bounds__(256) stream_only_kernel(SimParams P, FastDiv dnx, FastDiv dnxy,
+__global__ void __launch_bounds__(256) stream_only_kernel(const __grid_constant__ SimParams P, FastDiv dnx, FastDiv dnxy,
                                                           const S* __restrict__ fin,
                                                           S* __restrict__ fout,
                                                           const R* __restrict__ rho_buf) {
@@ -200,7 +218,7 @@ __global__ void __launch_bounds__(256) stream_only_kernel(SimParams P, FastDiv d
     q.x = (int)(r - (uint32_t)q.y * (uint32_t)P.nx);
     const bool mv = P.moving_any && touches_moving(P, q.x, q.y, q.z);
     R f[15];
-    gather<R, S>(P, fin, c, q, mv ? rho_buf[c] : R(0), f);
+    gather<R, S>(P, phys_ref<R>(P), fin, c, q, mv ? rho_buf[c] : R(0), f);
 #pragma unroll
     for (int j = 0; j < 15; ++j) Store<S>::st(fout + j * P.V + c, f[j]);
 }
@@ -214,7 +232,7 @@ __global__ void __launch_bounds__(256) feq_init_kernel(SimParams P, const R* __r
     const int64_t V = P.V;
     const R r = rho[c], ux = u[c], uy = u[V + c], uz = u[2 * V + c];
     const R u2 = ux * ux + uy * uy + uz * uz;
-    const R rho0 = R(P.kDensity);
+    const R rho0 = phys_ref<R>(P).kDensity;
 #pragma unroll
     for (int j = 0; j < 15; ++j) {
         const R w = w_<R>(j);

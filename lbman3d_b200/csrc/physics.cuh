@@ -6,7 +6,8 @@
 // (src/model.h:102-361, src/physics_helpers.h:69-129,
 // src/boundary_handler.h:112-392), so its results are bitwise equal to the
 // reference CPU solver.  The FP32 instantiation is the same algebra with
-// contraction allowed.
+// contraction allowed.  Halving is written as a multiplication by 0.5, which
+// is exact and therefore identical to the reference's division by 2.0.
 #pragma once
 
 #include "common.cuh"
@@ -19,56 +20,89 @@ struct QD {
     R dx, dy, dz, lap, d2x, d2y, d2z;
 };
 
-// Neighbour pair for one Q component along one axis.  m_img / p_img are the
-// values stored at the periodic image positions a-1 / a+1 (always present in
-// the staged tile); the rule below picks them, the centre (clamp) or the
-// anchoring ghost exactly like SafeFetchAxisOffset + QAxisGhostPair
-// (src/boundary_handler.h:76-89, 253-282).
-template <class R>
-__device__ __forceinline__ void q_pair(const SimParams& P, int ax, int comp, int a, int n, R m_img,
-                                       R c, R p_img, R& m, R& p) {
-    const int lo = 2 * ax, hi = lo + 1;
-    m = (a == 0 && !P.qper[lo]) ? c : m_img;
-    p = (a == n - 1 && !P.qper[hi]) ? c : p_img;
-    if (!P.qper[lo]) {  // the Lo tag decides whether ghosts apply on this axis
-        if (a == 0) m = P.face[lo].qbc == Q_ANCHORING ? R(2.0) * R(P.face[lo].anchor[comp]) - c : c;
-        if (a == n - 1) p = P.face[hi].qbc == Q_ANCHORING ? R(2.0) * R(P.face[hi].anchor[comp]) - c : c;
+// Wall handling of one axis at one point, decided once per point and reused
+// for every component: SafeFetchAxisOffset + QAxisGhostPair for Q
+// (src/boundary_handler.h:76-89, 253-282), VelocityAxisGhostPair for u
+// (src/boundary_handler.h:135-146).
+struct AxisRule {
+    bool m_clamp, p_clamp;    // take the centre value instead of the image
+    bool m_ghost, p_ghost;    // then replace by the face's ghost rule
+    int lo, hi;               // face indices
+};
+
+__device__ __forceinline__ AxisRule q_rule(const SimParams& P, int ax, int a, int n) {
+    AxisRule r;
+    r.lo = 2 * ax;
+    r.hi = r.lo + 1;
+    r.m_clamp = a == 0 && !P.qper[r.lo];
+    r.p_clamp = a == n - 1 && !P.qper[r.hi];
+    // the Lo tag decides whether ghosts apply on this axis
+    r.m_ghost = !P.qper[r.lo] && a == 0 && P.face[r.lo].qbc == Q_ANCHORING;
+    r.p_ghost = !P.qper[r.lo] && a == n - 1 && P.face[r.hi].qbc == Q_ANCHORING;
+    // a Neumann (or Periodic-tagged) ghost equals the centre, i.e. a clamp
+    if (!P.qper[r.lo]) {
+        if (a == 0) r.m_clamp = true;
+        if (a == n - 1) r.p_clamp = true;
     }
+    return r;
+}
+
+template <class R>
+__device__ __forceinline__ void q_apply(const AxisRule& r, const Phys<R>& K, int comp, R c, R& m, R& p) {
+    if (r.m_clamp) m = c;
+    if (r.p_clamp) p = c;
+    if (r.m_ghost) m = R(2.0) * K.anchor[r.lo][comp] - c;
+    if (r.p_ghost) p = R(2.0) * K.anchor[r.hi][comp] - c;
+}
+
+struct VRule {
+    bool m_clamp, p_clamp, m_wall, p_wall;
+    int lo, hi;
+};
+
+__device__ __forceinline__ VRule v_rule(const SimParams& P, int ax, int a, int n) {
+    VRule r;
+    r.lo = 2 * ax;
+    r.hi = r.lo + 1;
+    r.m_clamp = a == 0 && !P.uper[r.lo];
+    r.p_clamp = a == n - 1 && !P.uper[r.hi];
+    r.m_wall = !P.uper[r.lo] && a == 0;
+    r.p_wall = !P.uper[r.lo] && a == n - 1;
+    return r;
+}
+
+// VelocityGhost (src/boundary_handler.h:121-130).
+template <class R>
+__device__ __forceinline__ R v_ghost(const SimParams& P, const Phys<R>& K, int face, int comp, R vb,
+                                     bool normal) {
+    const int ubc = P.face[face].ubc;
+    const R wall = ubc == U_MOVING ? K.uw[face][comp] : R(0.0);
+    if (ubc == U_SPECULAR) return normal ? (R(2.0) * wall - vb) : vb;
+    return R(2.0) * wall - vb;
+}
+
+// VelocityAxisGradient (src/boundary_handler.h:157-163).
+template <class R>
+__device__ __forceinline__ R v_grad(const SimParams& P, const Phys<R>& K, const VRule& r, int comp, R m,
+                                    R c, R p, bool normal) {
+    if (r.m_clamp) m = c;
+    if (r.p_clamp) p = c;
+    if (r.m_wall) m = v_ghost<R>(P, K, r.lo, comp, c, normal);
+    if (r.p_wall) p = v_ghost<R>(P, K, r.hi, comp, c, normal);
+    return R(0.5) * (p - m);
 }
 
 template <class R>
 __device__ __forceinline__ QD<R> q_derivs(R xm, R xp, R ym, R yp, R zm, R zp, R c) {
     QD<R> d;
-    d.dx = (xp - xm) / R(2.0);
-    d.dy = (yp - ym) / R(2.0);
-    d.dz = (zp - zm) / R(2.0);
+    d.dx = R(0.5) * (xp - xm);
+    d.dy = R(0.5) * (yp - ym);
+    d.dz = R(0.5) * (zp - zm);
     d.lap = (xm + xp + ym + yp + zm + zp) - R(6.0) * c;
     d.d2x = (xm + xp) - R(2.0) * c;
     d.d2y = (ym + yp) - R(2.0) * c;
     d.d2z = (zm + zp) - R(2.0) * c;
     return d;
-}
-
-// VelocityGhost / VelocityAxisGradient (src/boundary_handler.h:121-163).
-template <class R>
-__device__ __forceinline__ R v_ghost(const SimParams& P, int face, int comp, R vb, bool normal) {
-    const Face& f = P.face[face];
-    const R wall = f.ubc == U_MOVING ? R(f.uw[comp]) : R(0.0);
-    if (f.ubc == U_SPECULAR) return normal ? (R(2.0) * wall - vb) : vb;
-    return R(2.0) * wall - vb;
-}
-
-template <class R>
-__device__ __forceinline__ R v_grad(const SimParams& P, int ax, int comp, int a, int n, R m_img, R c,
-                                    R p_img, bool normal) {
-    const int lo = 2 * ax, hi = lo + 1;
-    R m = (a == 0 && !P.uper[lo]) ? c : m_img;
-    R p = (a == n - 1 && !P.uper[hi]) ? c : p_img;
-    if (!P.uper[lo]) {
-        if (a == 0) m = v_ghost<R>(P, lo, comp, c, normal);
-        if (a == n - 1) p = v_ghost<R>(P, hi, comp, c, normal);
-    }
-    return (p - m) / R(2.0);
 }
 
 template <class R>
@@ -94,11 +128,10 @@ __device__ __forceinline__ R adv_deriv(R ux, R uy, R uz, const QD<R>& d) {
 // PointwiseStepAndSetupBodyForce (src/model.h:102-342): Q_new, Sigma, tau and
 // the Ericksen force -H:grad Q at one cell.
 template <class R, bool UPWIND>
-__device__ __forceinline__ void pointwise_q(const SimParams& P, const R Q[5], R ux, R uy, R uz,
+__device__ __forceinline__ void pointwise_q(const Phys<R>& K, const R Q[5], R ux, R uy, R uz,
                                             const QD<R> d[5], const GradU<R>& g, R qn[5], R sig[5],
                                             R tau[3], R eric[3]) {
-    const R A = R(P.A), B = R(P.B), C = R(P.C), L = R(P.L), LAMBDA = R(P.LAMBDA),
-            GAMMA = R(P.GAMMA), DT = R(P.DT);
+    const R A = K.A, B = K.B, C = K.C, L = K.L, LAMBDA = K.LAMBDA, GAMMA = K.GAMMA, DT = K.DT;
     const R Qxx = Q[0], Qxy = Q[1], Qxz = Q[2], Qyy = Q[3], Qyz = Q[4];
 
     const R TrQ2 = R(2.0) * (Qxx * Qxx + Qyy * Qyy + Qxx * Qyy + Qxy * Qxy + Qxz * Qxz + Qyz * Qyz);
@@ -194,10 +227,10 @@ __device__ __forceinline__ void pointwise_q(const SimParams& P, const R Q[5], R 
 // the Ericksen seed.  dS[axis][comp] are the centred differences of the 5
 // Sigma components, dT[axis][comp] of the 3 tau components.
 template <class R>
-__device__ __forceinline__ void active_passive_force(const SimParams& P, const R dQ[5][3],
-                                                     const R dS[3][5], const R dT[3][3], R ux, R uy,
-                                                     R uz, const R eric[3], R F[3]) {
-    const R ALPHA = R(P.ALPHA), MU = R(P.MU);
+__device__ __forceinline__ void active_passive_force(const Phys<R>& K, const R dQ[5][3], const R dS[3][5],
+                                                     const R dT[3][3], R ux, R uy, R uz, const R eric[3],
+                                                     R F[3]) {
+    const R ALPHA = K.ALPHA, MU = K.MU;
     // f_x = d_x S_xx + d_y(S_xy + T_xy) + d_z(S_xz + T_xz), ... (row convention)
     const R dz_Szz = -(dS[2][0] + dS[2][3]);
     const R pdx = dS[0][0] + (dS[1][1] + dT[1][0]) + (dS[2][2] + dT[2][1]);

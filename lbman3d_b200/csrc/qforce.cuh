@@ -1,30 +1,44 @@
-// qforce.cuh -- one kernel for the whole Q-tensor half of a time step:
+// qforce.cuh -- the whole Q-tensor half of a time step in one pass:
 // QTensorSolver::StepAndSetupBodyForce followed by
 // SetActiveStressAndComputeBodyForce (src/qtensor_solver.tpp:51-217), i.e.
 // the reference's GpuQTensorStep + GpuComputeBodyForce pair
-// (src/cuda/kernels.cu:122-292) in a single pass.
+// (src/cuda/kernels.cu:122-292).
 //
-// Each block owns a tcx x tcy tile of the x-y plane and marches through a
-// chunk of z planes.  Q and u (8 values per cell) are staged in shared
-// memory as a ring of three planes with a 2-cell x-y halo; the per-cell
-// results Q_new, Sigma, tau and the Ericksen force (16 values) are kept as a
-// ring of three planes with a 1-cell halo.  The stress divergence and the
-// gradient of Q_new are then taken from shared memory, so Sigma, tau, Q_new
-// and the Ericksen seed never travel through HBM: per cell the kernel reads
-// Q, u once and writes Q_new and the body force F once (16 words), instead
-// of the reference's 46 words across two kernels.
+// Each block owns a TCX x TCY tile of the x-y plane and marches through a
+// chunk of z planes.  Q and u (8 values per cell) are staged in shared memory
+// as a ring of four planes with a 2-cell x-y halo, filled by cp.async one
+// plane ahead; the per-point results Q_new, Sigma and tau (13 values) are kept
+// as a ring of three planes with a 1-cell halo.  One thread owns one point of
+// the halo tile: it computes that point's Beris-Edwards update for every
+// plane, keeps its Ericksen force in registers, and -- if the point is a tile
+// cell -- takes the stress divergence and grad Q_new from shared memory and
+// hands the cell's Q_new, body force and u to the consumer (global stores, or
+// the collide/stream of the fused kernel).  Sigma, tau, Q_new and the
+// Ericksen seed never travel through HBM.
 //
-// Halo cells are loaded with periodic wrap on every axis; the wall rules
-// then choose between the wrapped image, the centre value (clamp) and the
-// anchoring ghost exactly as the reference's index/ghost policies do, so a
-// wrapped value is only ever used on a periodic side.
+// Halo values are loaded with periodic wrap on every axis; the wall rules
+// choose between the wrapped image, the centre value (clamp) and the
+// anchoring ghost exactly as the reference's index/ghost policies do.  Blocks
+// whose halo touches no wall skip the rules altogether (block-uniform test).
 #pragma once
 
 #include "physics.cuh"
 
 namespace lbman {
 
-// Ring slots: results (B) keep 3 planes, staged Q/u keep 4 (one is in flight).
+template <int TCX_, int TCY_>
+struct Tile {
+    static constexpr int TCX = TCX_, TCY = TCY_;
+    static constexpr int BX = TCX + 2, BY = TCY + 2, NB = BX * BY;  // halo-1 result region
+    static constexpr int UX = TCX + 4, UY = TCY + 4, NQU = UX * UY;  // halo-2 staged region
+    static constexpr int NT = (NB + 31) / 32 * 32;                   // threads per block
+    static constexpr int NBV = 13;                                   // Q_new 5, Sigma 5, tau 3
+    template <class R>
+    static constexpr size_t smem_bytes() {
+        return sizeof(R) * (size_t)(4 * 8 * NQU + 3 * NBV * NB);
+    }
+};
+
 __device__ __forceinline__ int ring3(int z, int z0) { return (z - z0 + 6) % 3; }
 __device__ __forceinline__ int ring4(int z, int z0) { return (z - z0 + 8) & 3; }
 
@@ -40,198 +54,239 @@ __device__ __forceinline__ void cp_async(double* s, const double* g) {
 __device__ __forceinline__ void cp_async_wait_all() { asm volatile("cp.async.wait_all;\n" ::: "memory"); }
 
 // Issue the copies of plane zg (Q then u, tile + 2-cell halo, periodic wrap)
-// into its ring slot.  Completes at the next cp_async_wait_all().
-template <class R>
-__device__ __forceinline__ void qf_load_plane(const SimParams& P, const QTile& T, int x0, int y0,
-                                              int z0, int zg, const R* __restrict__ qin,
-                                              const R* __restrict__ uin, R* QU) {
-    const int uxw = T.tcx + 4, uyw = T.tcy + 4, nQU = uxw * uyw;
+// into its ring slot; complete at the next cp_async_wait_all().
+template <class TL, class R>
+__device__ __forceinline__ void qf_load_plane(const SimParams& P, int x0, int y0, int z0, int zg,
+                                              const R* __restrict__ qin, const R* __restrict__ uin, R* QU) {
     const int zw = wrap_coord(zg, P.nz);
-    R* dst = QU + ring4(zg, z0) * 8 * nQU;
-    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, nwarp = blockDim.x >> 5;
+    R* dst = QU + ring4(zg, z0) * 8 * TL::NQU;
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    constexpr int nwarp = TL::NT / 32;
     const int64_t zoff = (int64_t)zw * P.nxy;
-    for (int row = warp; row < 8 * uyw; row += nwarp) {
-        const int var = row / uyw, ly = row - var * uyw;
+#pragma unroll 1
+    for (int row = warp; row < 8 * TL::UY; row += nwarp) {
+        const int var = row / TL::UY, ly = row - var * TL::UY;
         const int gy = wrap_coord(y0 - 2 + ly, P.ny);
         const R* src = (var < 5 ? qin + (int64_t)var * P.V : uin + (int64_t)(var - 5) * P.V) + zoff +
                        (int64_t)gy * P.nx;
-        R* d = dst + var * nQU + ly * uxw;
-        for (int lx = lane; lx < uxw; lx += 32) cp_async(d + lx, src + wrap_coord(x0 - 2 + lx, P.nx));
+        R* d = dst + var * TL::NQU + ly * TL::UX;
+#pragma unroll
+        for (int lx = lane; lx < TL::UX; lx += 32) cp_async(d + lx, src + wrap_coord(x0 - 2 + lx, P.nx));
     }
 }
 
-template <class R, bool UPWIND>
-__device__ __forceinline__ void qf_compute_plane(const SimParams& P, const QTile& T, int x0, int y0,
-                                                 int z0, int zb, const R* QU, R* Bs) {
-    const int uxw = T.tcx + 4, uyw = T.tcy + 4, nQU = uxw * uyw;
-    const int bxw = T.tcx + 2, byw = T.tcy + 2, nB = bxw * byw;
-    const R* Qc = QU + ring4(zb, z0) * 8 * nQU;
-    const R* Qm = QU + ring4(zb - 1, z0) * 8 * nQU;
-    const R* Qp = QU + ring4(zb + 1, z0) * 8 * nQU;
-    R* Bd = Bs + ring3(zb, z0) * 16 * nB;
-    const int az = wrap_coord(zb, P.nz);
-    for (int p = threadIdx.x; p < nB; p += blockDim.x) {
-        const int lby = p / bxw, lbx = p - lby * bxw;
-        const int ax = wrap_coord(x0 - 1 + lbx, P.nx), ay = wrap_coord(y0 - 1 + lby, P.ny);
-        const int up = (lby + 1) * uxw + lbx + 1;
-        R Q[5];
-        QD<R> d[5];
-#pragma unroll
-        for (int k = 0; k < 5; ++k) {
-            const R* qc = Qc + k * nQU;
-            const R c = qc[up];
-            R xm, xp, ym, yp, zm, zp;
-            q_pair<R>(P, 0, k, ax, P.nx, qc[up - 1], c, qc[up + 1], xm, xp);
-            q_pair<R>(P, 1, k, ay, P.ny, qc[up - uxw], c, qc[up + uxw], ym, yp);
-            q_pair<R>(P, 2, k, az, P.nz, Qm[k * nQU + up], c, Qp[k * nQU + up], zm, zp);
-            d[k] = q_derivs<R>(xm, xp, ym, yp, zm, zp, c);
-            Q[k] = c;
-        }
-        const R* uxc = Qc + 5 * nQU;
-        const R* uyc = Qc + 6 * nQU;
-        const R* uzc = Qc + 7 * nQU;
-        const R ux0 = uxc[up], uy0 = uyc[up], uz0 = uzc[up];
-        GradU<R> g;
-        g.ux_x = v_grad<R>(P, 0, 0, ax, P.nx, uxc[up - 1], ux0, uxc[up + 1], true);
-        g.ux_y = v_grad<R>(P, 1, 0, ay, P.ny, uxc[up - uxw], ux0, uxc[up + uxw], false);
-        g.ux_z = v_grad<R>(P, 2, 0, az, P.nz, Qm[5 * nQU + up], ux0, Qp[5 * nQU + up], false);
-        g.uy_x = v_grad<R>(P, 0, 1, ax, P.nx, uyc[up - 1], uy0, uyc[up + 1], false);
-        g.uy_y = v_grad<R>(P, 1, 1, ay, P.ny, uyc[up - uxw], uy0, uyc[up + uxw], true);
-        g.uy_z = v_grad<R>(P, 2, 1, az, P.nz, Qm[6 * nQU + up], uy0, Qp[6 * nQU + up], false);
-        g.uz_x = v_grad<R>(P, 0, 2, ax, P.nx, uzc[up - 1], uz0, uzc[up + 1], false);
-        g.uz_y = v_grad<R>(P, 1, 2, ay, P.ny, uzc[up - uxw], uz0, uzc[up + uxw], false);
-        R qn[5], sg[5], ta[3], er[3];
-        pointwise_q<R, UPWIND>(P, Q, ux0, uy0, uz0, d, g, qn, sg, ta, er);
-#pragma unroll
-        for (int k = 0; k < 5; ++k) Bd[k * nB + p] = qn[k];
-#pragma unroll
-        for (int k = 0; k < 5; ++k) Bd[(5 + k) * nB + p] = sg[k];
-#pragma unroll
-        for (int k = 0; k < 3; ++k) Bd[(10 + k) * nB + p] = ta[k];
-#pragma unroll
-        for (int k = 0; k < 3; ++k) Bd[(13 + k) * nB + p] = er[k];
-    }
+// Per-thread geometry, fixed for the whole z march.
+struct PointGeo {
+    int lbx, lby;     // position in the result region
+    int ax, ay;       // wrapped global coordinates of the point
+    bool hasB, isC;   // owns a result point / a tile cell
+    bool wx, wy, wz;  // block-uniform: wall rules may apply on this axis
+};
+
+template <class TL>
+__device__ __forceinline__ PointGeo point_geo(const SimParams& P, int x0, int y0, int z0, int z1) {
+    PointGeo g;
+    const int t = threadIdx.x;
+    g.hasB = t < TL::NB;
+    g.lbx = t % TL::BX;
+    g.lby = t / TL::BX;
+    g.ax = wrap_coord(x0 - 1 + g.lbx, P.nx);
+    g.ay = wrap_coord(y0 - 1 + g.lby, P.ny);
+    g.isC = g.hasB && g.lbx >= 1 && g.lbx <= TL::TCX && g.lby >= 1 && g.lby <= TL::TCY &&
+            x0 + g.lbx - 1 < P.nx && y0 + g.lby - 1 < P.ny;
+    const bool perx = P.qper[0] && P.qper[1] && P.uper[0] && P.uper[1];
+    const bool pery = P.qper[2] && P.qper[3] && P.uper[2] && P.uper[3];
+    const bool perz = P.qper[4] && P.qper[5] && P.uper[4] && P.uper[5];
+    g.wx = !perx && (x0 - 1 < 1 || x0 + TL::TCX > P.nx - 2);
+    g.wy = !pery && (y0 - 1 < 1 || y0 + TL::TCY > P.ny - 2);
+    g.wz = !perz && (z0 - 1 < 1 || z1 > P.nz - 2);
+    return g;
 }
 
-// Body force at the tile cells of plane zc, from the staged B planes.
-// OutFn(cell, x, y, z, qn[5], F[3], u[3]) consumes the result (stores it, or
-// runs the collide/stream step on it in the fused kernel).
-template <class R, class OutFn>
-__device__ __forceinline__ void qf_force_plane(const SimParams& P, const QTile& T, int x0, int y0,
-                                               int z0, int zc, const R* QU, const R* Bs, OutFn&& out) {
-    const int uxw = T.tcx + 4, uyw = T.tcy + 4, nQU = uxw * uyw;
-    const int bxw = T.tcx + 2, byw = T.tcy + 2, nB = bxw * byw;
-    const R* B0 = Bs + ring3(zc, z0) * 16 * nB;
-    const R* Bm = Bs + ring3(zc - 1, z0) * 16 * nB;
-    const R* Bp = Bs + ring3(zc + 1, z0) * 16 * nB;
-    const R* U0 = QU + ring4(zc, z0) * 8 * nQU;
-    const int ntile = T.tcx * T.tcy;
-    for (int p = threadIdx.x; p < ntile; p += blockDim.x) {
-        const int lcy = p / T.tcx, lcx = p - lcy * T.tcx;
-        const int gx = x0 + lcx, gy = y0 + lcy;
-        if (gx >= P.nx || gy >= P.ny) continue;
-        const int bp = (lcy + 1) * bxw + lcx + 1;
-        // grad Q_new with the wall ghosts (QGradientAndLaplacian on the new Q).
-        R dQ[5][3];
-        R qn[5];
-#pragma unroll
-        for (int k = 0; k < 5; ++k) {
-            const R* b = B0 + k * nB;
-            const R c = b[bp];
-            qn[k] = c;
-            R m, q;
-            q_pair<R>(P, 0, k, gx, P.nx, b[bp - 1], c, b[bp + 1], m, q);
-            dQ[k][0] = (q - m) / R(2.0);
-            q_pair<R>(P, 1, k, gy, P.ny, b[bp - bxw], c, b[bp + bxw], m, q);
-            dQ[k][1] = (q - m) / R(2.0);
-            q_pair<R>(P, 2, k, zc, P.nz, Bm[k * nB + bp], c, Bp[k * nB + bp], m, q);
-            dQ[k][2] = (q - m) / R(2.0);
-        }
-        // Sigma / tau differences with the Neumann/periodic index clamp QXoff
-        // (src/offsets.h:59-83, used by PassiveStressDivergence).
-        const bool xmc = gx == 0 && !P.qper[0], xpc = gx == P.nx - 1 && !P.qper[1];
-        const bool ymc = gy == 0 && !P.qper[2], ypc = gy == P.ny - 1 && !P.qper[3];
-        const bool zmc = zc == 0 && !P.qper[4], zpc = zc == P.nz - 1 && !P.qper[5];
-        R dS[3][5], dT[3][3];
-#pragma unroll
-        for (int v = 0; v < 8; ++v) {
-            const R* b = B0 + (5 + v) * nB;
-            const R c = b[bp];
-            const R xm = xmc ? c : b[bp - 1], xp = xpc ? c : b[bp + 1];
-            const R ym = ymc ? c : b[bp - bxw], yp = ypc ? c : b[bp + bxw];
-            const R zm = zmc ? c : Bm[(5 + v) * nB + bp], zp = zpc ? c : Bp[(5 + v) * nB + bp];
-            const R ddx = (xp - xm) / R(2.0), ddy = (yp - ym) / R(2.0), ddz = (zp - zm) / R(2.0);
-            if (v < 5) { dS[0][v] = ddx; dS[1][v] = ddy; dS[2][v] = ddz; }
-            else { dT[0][v - 5] = ddx; dT[1][v - 5] = ddy; dT[2][v - 5] = ddz; }
-        }
-        const int uq = (lcy + 2) * uxw + lcx + 2;
-        const R u[3] = {U0[5 * nQU + uq], U0[6 * nQU + uq], U0[7 * nQU + uq]};
-        const R er[3] = {B0[13 * nB + bp], B0[14 * nB + bp], B0[15 * nB + bp]};
-        R F[3];
-        active_passive_force<R>(P, dQ, dS, dT, u[0], u[1], u[2], er, F);
-        const int64_t cell = (int64_t)zc * P.nxy + (int64_t)gy * P.nx + gx;
-        out(cell, gx, gy, zc, qn, F, u);
+// Beris-Edwards update of this thread's point in plane zb; results to the
+// ring slot of zb, Ericksen force to er.
+template <class TL, class R, bool UPWIND>
+__device__ __forceinline__ void qf_compute_plane(const SimParams& P, const Phys<R>& K, const PointGeo& G,
+                                                 const AxisRule& qx, const AxisRule& qy, const VRule& vx,
+                                                 const VRule& vy, int z0, int zb, const R* QU, R* Bs,
+                                                 R er[3]) {
+    if (!G.hasB) return;
+    constexpr int NQU = TL::NQU, UX = TL::UX, NB = TL::NB;
+    const R* Qc = QU + ring4(zb, z0) * 8 * NQU;
+    const R* Qm = QU + ring4(zb - 1, z0) * 8 * NQU;
+    const R* Qp = QU + ring4(zb + 1, z0) * 8 * NQU;
+    const int up = (G.lby + 1) * UX + G.lbx + 1;
+    AxisRule qz;
+    VRule vz;
+    if (G.wz) {
+        const int az = wrap_coord(zb, P.nz);
+        qz = q_rule(P, 2, az, P.nz);
+        vz = v_rule(P, 2, az, P.nz);
     }
+    R Q[5];
+    QD<R> d[5];
+#pragma unroll
+    for (int k = 0; k < 5; ++k) {
+        const R* qc = Qc + k * NQU;
+        const R c = qc[up];
+        R xm = qc[up - 1], xp = qc[up + 1], ym = qc[up - UX], yp = qc[up + UX];
+        R zm = Qm[k * NQU + up], zp = Qp[k * NQU + up];
+        if (G.wx) q_apply<R>(qx, K, k, c, xm, xp);
+        if (G.wy) q_apply<R>(qy, K, k, c, ym, yp);
+        if (G.wz) q_apply<R>(qz, K, k, c, zm, zp);
+        d[k] = q_derivs<R>(xm, xp, ym, yp, zm, zp, c);
+        Q[k] = c;
+    }
+    const R* uc[3] = {Qc + 5 * NQU, Qc + 6 * NQU, Qc + 7 * NQU};
+    const R u0[3] = {uc[0][up], uc[1][up], uc[2][up]};
+    // (component, axis) pairs of the stored gradient: ux_x ux_y ux_z uy_x uy_y uy_z uz_x uz_y
+    R gr[8];
+#pragma unroll
+    for (int comp = 0; comp < 3; ++comp) {
+        const R c = u0[comp];
+        const R xm = uc[comp][up - 1], xp = uc[comp][up + 1];
+        const R ym = uc[comp][up - UX], yp = uc[comp][up + UX];
+        gr[comp * 3 + 0] = G.wx ? v_grad<R>(P, K, vx, comp, xm, c, xp, comp == 0) : R(0.5) * (xp - xm);
+        gr[comp * 3 + 1] = G.wy ? v_grad<R>(P, K, vy, comp, ym, c, yp, comp == 1) : R(0.5) * (yp - ym);
+        if (comp < 2) {
+            const R zm = Qm[(5 + comp) * NQU + up], zp = Qp[(5 + comp) * NQU + up];
+            gr[comp * 3 + 2] = G.wz ? v_grad<R>(P, K, vz, comp, zm, c, zp, false) : R(0.5) * (zp - zm);
+        }
+    }
+    GradU<R> g;
+    g.ux_x = gr[0]; g.ux_y = gr[1]; g.ux_z = gr[2];
+    g.uy_x = gr[3]; g.uy_y = gr[4]; g.uy_z = gr[5];
+    g.uz_x = gr[6]; g.uz_y = gr[7];
+    R qn[5], sg[5], ta[3];
+    pointwise_q<R, UPWIND>(K, Q, u0[0], u0[1], u0[2], d, g, qn, sg, ta, er);
+    R* Bd = Bs + ring3(zb, z0) * TL::NBV * NB + threadIdx.x;
+#pragma unroll
+    for (int k = 0; k < 5; ++k) Bd[k * NB] = qn[k];
+#pragma unroll
+    for (int k = 0; k < 5; ++k) Bd[(5 + k) * NB] = sg[k];
+#pragma unroll
+    for (int k = 0; k < 3; ++k) Bd[(10 + k) * NB] = ta[k];
 }
 
-// Marches a block through its z chunk; PlaneOut is called once per output
-// plane after the staged planes are complete.  The copy of plane zc+3 is in
-// flight while planes zc+1 (results) and zc (force, output) are computed, so
-// the global-memory latency of the staging is hidden behind the arithmetic.
-template <class R, bool UPWIND, class PlaneOut>
-__device__ __forceinline__ void qf_march(const SimParams& P, const QTile& T,
-                                         const R* __restrict__ qin, const R* __restrict__ uin,
-                                         R* QU, R* Bs, PlaneOut&& plane_out) {
-    const int x0 = blockIdx.x * T.tcx, y0 = blockIdx.y * T.tcy;
-    const int z0 = blockIdx.z * T.zc;
+// Body force of this thread's tile cell in plane zc from the staged result
+// planes; out(cell, x, y, z, qn[5], F[3], u[3]) consumes it.
+template <class TL, class R, class OutFn>
+__device__ __forceinline__ void qf_force_cell(const SimParams& P, const Phys<R>& K, const PointGeo& G,
+                                              const AxisRule& qx, const AxisRule& qy, int x0, int y0, int z0,
+                                              int zc, const R* QU, const R* Bs, const R er[3], OutFn&& out) {
+    if (!G.isC) return;
+    constexpr int NB = TL::NB, BX = TL::BX, NBV = TL::NBV;
+    const int t = threadIdx.x;
+    const R* B0 = Bs + ring3(zc, z0) * NBV * NB;
+    const R* Bm = Bs + ring3(zc - 1, z0) * NBV * NB;
+    const R* Bp = Bs + ring3(zc + 1, z0) * NBV * NB;
+    const int gx = x0 + G.lbx - 1, gy = y0 + G.lby - 1;
+    AxisRule qz;
+    if (G.wz) qz = q_rule(P, 2, zc, P.nz);
+    // grad Q_new with the wall ghosts (QGradientAndLaplacian on the new Q)
+    R dQ[5][3], qn[5];
+#pragma unroll
+    for (int k = 0; k < 5; ++k) {
+        const R* b = B0 + k * NB;
+        const R c = b[t];
+        qn[k] = c;
+        R xm = b[t - 1], xp = b[t + 1], ym = b[t - BX], yp = b[t + BX];
+        R zm = Bm[k * NB + t], zp = Bp[k * NB + t];
+        if (G.wx) q_apply<R>(qx, K, k, c, xm, xp);
+        if (G.wy) q_apply<R>(qy, K, k, c, ym, yp);
+        if (G.wz) q_apply<R>(qz, K, k, c, zm, zp);
+        dQ[k][0] = R(0.5) * (xp - xm);
+        dQ[k][1] = R(0.5) * (yp - ym);
+        dQ[k][2] = R(0.5) * (zp - zm);
+    }
+    // Sigma / tau differences with the Neumann/periodic index clamp QXoff
+    // (src/offsets.h:59-83, used by PassiveStressDivergence).
+    const bool xmc = G.wx && gx == 0 && !P.qper[0], xpc = G.wx && gx == P.nx - 1 && !P.qper[1];
+    const bool ymc = G.wy && gy == 0 && !P.qper[2], ypc = G.wy && gy == P.ny - 1 && !P.qper[3];
+    const bool zmc = G.wz && zc == 0 && !P.qper[4], zpc = G.wz && zc == P.nz - 1 && !P.qper[5];
+    R dS[3][5], dT[3][3];
+#pragma unroll
+    for (int v = 0; v < 8; ++v) {
+        const R* b = B0 + (5 + v) * NB;
+        const R c = b[t];
+        const R xm = xmc ? c : b[t - 1], xp = xpc ? c : b[t + 1];
+        const R ym = ymc ? c : b[t - BX], yp = ypc ? c : b[t + BX];
+        const R zm = zmc ? c : Bm[(5 + v) * NB + t], zp = zpc ? c : Bp[(5 + v) * NB + t];
+        const R ddx = R(0.5) * (xp - xm), ddy = R(0.5) * (yp - ym), ddz = R(0.5) * (zp - zm);
+        if (v < 5) { dS[0][v] = ddx; dS[1][v] = ddy; dS[2][v] = ddz; }
+        else { dT[0][v - 5] = ddx; dT[1][v - 5] = ddy; dT[2][v - 5] = ddz; }
+    }
+    const R* U0 = QU + ring4(zc, z0) * 8 * TL::NQU;
+    const int up = (G.lby + 1) * TL::UX + G.lbx + 1;
+    const R u[3] = {U0[5 * TL::NQU + up], U0[6 * TL::NQU + up], U0[7 * TL::NQU + up]};
+    R F[3];
+    active_passive_force<R>(K, dQ, dS, dT, u[0], u[1], u[2], er, F);
+    const int64_t cell = (int64_t)zc * P.nxy + (int64_t)gy * P.nx + gx;
+    out(cell, gx, gy, zc, qn, F, u);
+}
+
+// Marches a block through its z chunk.  The copy of plane zc+3 is in flight
+// while planes zc+1 (results) and zc (force, consumer) are computed.
+template <class TL, class R, bool UPWIND, class OutFn>
+__device__ __forceinline__ void qf_march(const SimParams& P, int zc_len, const R* __restrict__ qin,
+                                         const R* __restrict__ uin, R* smem, OutFn&& out, int bx, int by,
+                                         int bz) {
+    R* QU = smem;
+    R* Bs = smem + 4 * 8 * TL::NQU;
+    const int x0 = bx * TL::TCX, y0 = by * TL::TCY;
+    const int z0 = bz * zc_len;
     if (z0 >= P.nz) return;
-    const int z1 = min(z0 + T.zc, P.nz);
-    for (int z = z0 - 2; z <= z0 + 1; ++z) qf_load_plane<R>(P, T, x0, y0, z0, z, qin, uin, QU);
+    const int z1 = min(z0 + zc_len, P.nz);
+    const Phys<R>& K = phys_ref<R>(P);
+    const PointGeo G = point_geo<TL>(P, x0, y0, z0, z1);
+    const AxisRule qx = q_rule(P, 0, G.ax, P.nx), qy = q_rule(P, 1, G.ay, P.ny);
+    const VRule vx = v_rule(P, 0, G.ax, P.nx), vy = v_rule(P, 1, G.ay, P.ny);
+    R er_cur[3], er_next[3];
+
+    for (int z = z0 - 2; z <= z0 + 1; ++z) qf_load_plane<TL>(P, x0, y0, z0, z, qin, uin, QU);
     cp_async_wait_all();
     __syncthreads();
-    qf_compute_plane<R, UPWIND>(P, T, x0, y0, z0, z0 - 1, QU, Bs);
-    qf_compute_plane<R, UPWIND>(P, T, x0, y0, z0, z0, QU, Bs);
-    __syncthreads();  // slot of z0-2 is free again
-    qf_load_plane<R>(P, T, x0, y0, z0, z0 + 2, qin, uin, QU);
+    qf_compute_plane<TL, R, UPWIND>(P, K, G, qx, qy, vx, vy, z0, z0 - 1, QU, Bs, er_next);
+    qf_compute_plane<TL, R, UPWIND>(P, K, G, qx, qy, vx, vy, z0, z0, QU, Bs, er_cur);
+    __syncthreads();  // the slot of z0-2 is free again
+    qf_load_plane<TL>(P, x0, y0, z0, z0 + 2, qin, uin, QU);
     cp_async_wait_all();
     __syncthreads();
+#pragma unroll 1
     for (int zc = z0; zc < z1; ++zc) {
-        // slot of zc-1 was last read by the previous iteration (before its final barrier)
-        if (zc + 1 < z1) qf_load_plane<R>(P, T, x0, y0, z0, zc + 3, qin, uin, QU);
-        qf_compute_plane<R, UPWIND>(P, T, x0, y0, z0, zc + 1, QU, Bs);
+        if (zc + 1 < z1) qf_load_plane<TL>(P, x0, y0, z0, zc + 3, qin, uin, QU);
+        qf_compute_plane<TL, R, UPWIND>(P, K, G, qx, qy, vx, vy, z0, zc + 1, QU, Bs, er_next);
         __syncthreads();
-        plane_out(x0, y0, z0, zc);
+        qf_force_cell<TL, R>(P, K, G, qx, qy, x0, y0, z0, zc, QU, Bs, er_cur, out);
+#pragma unroll
+        for (int k = 0; k < 3; ++k) er_cur[k] = er_next[k];
         cp_async_wait_all();
         __syncthreads();
     }
 }
 
+// Consumer of the split organisation: store Q_new and the body force.
 template <class R>
-__host__ __device__ inline int qf_qu_elems(const QTile& T) {
-    return 4 * 8 * (T.tcx + 4) * (T.tcy + 4);
-}
+struct StoreQForce {
+    R* __restrict__ qout;
+    R* __restrict__ Fout;
+    int64_t V;
+    __device__ __forceinline__ void operator()(int64_t cell, int, int, int, const R qn[5], const R F[3],
+                                               const R*) const {
+#pragma unroll
+        for (int k = 0; k < 5; ++k) qout[k * V + cell] = qn[k];
+#pragma unroll
+        for (int k = 0; k < 3; ++k) Fout[k * V + cell] = F[k];
+    }
+};
 
-template <class R, bool UPWIND>
-__global__ void __launch_bounds__(512) qforce_kernel(SimParams P, QTile T, const R* __restrict__ qin,
-                                                     const R* __restrict__ uin, R* __restrict__ qout,
-                                                     R* __restrict__ Fout) {
+template <class TL, class R, bool UPWIND>
+__global__ void __launch_bounds__(TL::NT) qforce_kernel(const __grid_constant__ SimParams P, int zc_len,
+                                                        const R* __restrict__ qin, const R* __restrict__ uin,
+                                                        R* __restrict__ qout, R* __restrict__ Fout) {
     extern __shared__ __align__(16) unsigned char smem_raw[];
-    R* QU = reinterpret_cast<R*>(smem_raw);
-    R* Bs = QU + qf_qu_elems<R>(T);
-    const int64_t V = P.V;
-    qf_march<R, UPWIND>(P, T, qin, uin, QU, Bs, [&](int x0, int y0, int z0, int zc) {
-        qf_force_plane<R>(P, T, x0, y0, z0, zc, QU, Bs,
-                          [&](int64_t cell, int, int, int, const R qn[5], const R F[3], const R*) {
-#pragma unroll
-                              for (int k = 0; k < 5; ++k) qout[k * V + cell] = qn[k];
-#pragma unroll
-                              for (int k = 0; k < 3; ++k) Fout[k * V + cell] = F[k];
-                          });
-    });
-}
-
-inline size_t qforce_smem_bytes(const QTile& T, size_t real_bytes) {
-    return real_bytes * (size_t)(4 * 8 * (T.tcx + 4) * (T.tcy + 4) + 3 * 16 * (T.tcx + 2) * (T.tcy + 2));
+    qf_march<TL, R, UPWIND>(P, zc_len, qin, uin, reinterpret_cast<R*>(smem_raw), StoreQForce<R>{qout, Fout, P.V},
+                            blockIdx.x, blockIdx.y, blockIdx.z);
 }
 
 }  // namespace lbman

@@ -130,6 +130,24 @@ class Simulation:
             N.check(st)
         return {k: getattr(d, k) for k, _ in N.lbman_diag._fields_}
 
+    def shape(self) -> dict:
+        s = N.lbman_shape()
+        N.check(N.lib().lbman_get_shape(self._h, C.byref(s)))
+        return {k: getattr(s, k) for k, _ in N.lbman_shape._fields_}
+
+    def set_shape(self, kernels: int, tile_x: int, tile_y: int, zchunk: int):
+        s = N.lbman_shape(kernels, tile_x, tile_y, zchunk, 0, 0.0)
+        N.check(N.lib().lbman_set_shape(self._h, C.byref(s)))
+
+    def autotune(self, steps_per_trial: int = 5) -> dict:
+        """Time every kernel organisation x tile x z-chunk candidate on the
+        current state, keep the fastest, restore the state."""
+        s, n = N.lbman_shape(), C.c_int()
+        N.check(N.lib().lbman_autotune(self._h, int(steps_per_trial), C.byref(s), C.byref(n)))
+        d = {k: getattr(s, k) for k, _ in N.lbman_shape._fields_}
+        d["trials"] = n.value
+        return d
+
     def launch_count(self) -> int:
         v = C.c_int64()
         N.check(N.lib().lbman_launch_count(self._h, C.byref(v)))

@@ -81,7 +81,7 @@ def test_fp64_bitwise_vs_oracle_larger_boxes(bc, grid, upwind, kernels):
     p, rho, u, q = _oracle_case(grid, BC[bc], upwind, ALPHA=0.015, MU=0.002)
     ref = O.OracleSim(p)
     ref.set(rho, u, q)
-    sim = sim_from(grid, BC[bc], dict(ALPHA=0.015, MU=0.002), upwind, kernels=kernels, tile=(14, 4, 5))
+    sim = sim_from(grid, BC[bc], dict(ALPHA=0.015, MU=0.002), upwind, kernels=kernels, tile=(14, 14, 5))
     sim.upload(rho, u, q)
     for n in (1, 7):
         ref.step(n)
