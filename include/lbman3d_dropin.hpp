@@ -29,6 +29,8 @@
 #include <params.h>
 #include <sim_config.h>
 
+#include <cmath>
+#include <random>
 #include <stdexcept>
 #include <string>
 #include <type_traits>
@@ -263,9 +265,13 @@ public:
     }
 };
 
-// GPU-backed QTensorSolver<BC> (src/qtensor_solver.h:23-52): Step runs
-// StepAndSetupBodyForce and SetActiveStressAndComputeBodyForce in one GPU
-// pass and writes the new Q and the full body force back to the host fields.
+// GPU-backed QTensorSolver<BC> (src/qtensor_solver.h:23-52).  One GPU pass
+// computes what the reference's StepAndSetupBodyForce followed by the base
+// SetActiveStressAndComputeBodyForce computes, and writes the new Q and the
+// full body force back to the host fields.  As in the reference's own GPU
+// path (src/active_nematic.h:85-86), an override of
+// SetActiveStressAndComputeBodyForce does not replace the built-in activity
+// model: it runs after the pass, on the full force.
 template <typename BC>
 class QTensorSolver {
     mutable lbman_solver* s_ = nullptr;
@@ -275,7 +281,38 @@ public:
     QTensorSolver(const QTensorSolver&) = delete;
     virtual ~QTensorSolver() { lbman_destroy(s_); }
 
+    // Host initialisation with the reference's semantics
+    // (src/qtensor_solver.tpp:14-48): director along z at the bulk order
+    // S_eq (src/model.h:39-41), plus U(-NOISE, NOISE) on every component from
+    // an unseeded generator.  Reproducible starts go through
+    // lbman_init_seeded or lbman_upload instead.
+    virtual void Initialize(QTensorFields& qf) const {
+        const double s_eq = (-Params::B + std::sqrt(Params::B * Params::B - 24.0 * Params::A * Params::C)) /
+                            (4.0 * Params::C);
+        std::random_device rd;
+        std::mt19937 gen(rd());
+        std::uniform_real_distribution<double> noise(-Params::NOISE, Params::NOISE);
+        const LocalGrid& g = qf.grid;
+        const int64_t V = (int64_t)g.local_nx * g.local_ny * g.local_nz;
+        for (int64_t c = 0; c < V; ++c) {
+            qf.qxx[c] = -s_eq / 3.0 + noise(gen);
+            qf.qxy[c] = noise(gen);
+            qf.qxz[c] = noise(gen);
+            qf.qyy[c] = -s_eq / 3.0 + noise(gen);
+            qf.qyz[c] = noise(gen);
+        }
+    }
+
+    void StepAndSetupBodyForce(QTensorFields& qf, FluidFields& ff) const { StepFused(qf, ff); }
+    virtual void SetActiveStressAndComputeBodyForce(FluidFields&, const QTensorFields&) const {}
+
     void Step(QTensorFields& qf, FluidFields& ff) const {
+        StepFused(qf, ff);
+        SetActiveStressAndComputeBodyForce(ff, qf);
+    }
+
+private:
+    void StepFused(QTensorFields& qf, FluidFields& ff) const {
         const LocalGrid& g = qf.grid;
         const int64_t V = (int64_t)g.local_nx * g.local_ny * g.local_nz;
         if (!s_) {

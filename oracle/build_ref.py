@@ -10,7 +10,10 @@ boundary configuration is chosen at run time by ref_driver.cc.
     python oracle/build_ref.py            # builds every set in REF_BUILDS
     python oracle/build_ref.py --list
 
-Outputs: oracle/_ref/<tag>/ref_driver (plus the generated headers).
+Outputs: oracle/_ref/<tag>/ref_driver (plus the generated headers), and
+oracle/_ref/<tag>/dropin_check for the DROPIN_BUILDS sets (the reference's
+solver classes beside include/lbman3d_dropin.hpp, linked against the built
+lbman3d_b200/liblbman3d_b200.so).
 """
 from __future__ import annotations
 
@@ -43,6 +46,12 @@ REF_BUILDS = {
     "b_slit": dict(nx=64, ny=256, nz=256, ALPHA=0.01),
     "b_channel": dict(nx=20, ny=100, nz=100, ALPHA=0.01),
     "b_p32": dict(nx=32, ny=32, nz=32),
+}
+
+# Parameter sets of the C++ drop-in check (dropin_check.cc, linked against
+# the built liblbman3d_b200.so).
+DROPIN_BUILDS = {
+    "d_box": dict(nx=10, ny=12, nz=8, ALPHA=0.02, MU=0.01),
 }
 
 
@@ -135,6 +144,34 @@ def build(tag: str, cfg: dict, verbose: bool = False) -> str:
     return exe
 
 
+def build_dropin(tag: str, cfg: dict, verbose: bool = False) -> str:
+    """dropin_check for one parameter set; needs lbman3d_b200/liblbman3d_b200.so."""
+    d = os.path.join(OUT, tag)
+    os.makedirs(d, exist_ok=True)
+    with open(os.path.join(d, "params.h"), "w") as fh:
+        fh.write(params_h(cfg))
+    with open(os.path.join(d, "sim_config.h"), "w") as fh:
+        fh.write(sim_config_h(cfg))
+    root = os.path.dirname(HERE)
+    pkg = os.path.join(root, "lbman3d_b200")
+    if not os.path.exists(os.path.join(pkg, "liblbman3d_b200.so")):
+        raise FileNotFoundError("build lbman3d_b200 first (python -m lbman3d_b200.build)")
+    exe = os.path.join(d, "dropin_check")
+    srcs = [os.path.join(HERE, "dropin_check.cc")] + [
+        os.path.join(REF_SRC, s) for s in ("fluid_fields.cc", "qtensor_fields.cc")]
+    cmd = ["g++", "-std=c++23", "-O3", "-DNDEBUG", "-fopenmp", "-w",
+           "-I", d, "-I", REF_SRC, "-I", os.path.join(root, "include"), "-o", exe] + srcs + [
+           "-L", pkg, "-llbman3d_b200", "-Wl,-rpath,$ORIGIN/../../../lbman3d_b200"]
+    if verbose:
+        print(" ".join(cmd))
+    subprocess.run(cmd, check=True)
+    return exe
+
+
+def dropin_path(tag: str) -> str:
+    return os.path.join(OUT, tag, "dropin_check")
+
+
 def driver_path(tag: str) -> str:
     return os.path.join(OUT, tag, "ref_driver")
 
@@ -149,10 +186,14 @@ def main(argv=None) -> int:
         for k, v in REF_BUILDS.items():
             print(k, v)
         return 0
-    tags = a.tags or list(REF_BUILDS)
+    tags = a.tags or list(REF_BUILDS) + list(DROPIN_BUILDS)
     for t in tags:
-        build(t, REF_BUILDS[t], a.v)
-        print("built", driver_path(t))
+        if t in DROPIN_BUILDS:
+            build_dropin(t, DROPIN_BUILDS[t], a.v)
+            print("built", dropin_path(t))
+        else:
+            build(t, REF_BUILDS[t], a.v)
+            print("built", driver_path(t))
     return 0
 
 
