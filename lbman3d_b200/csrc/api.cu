@@ -11,6 +11,7 @@
 
 #include "../../include/lbman3d.h"
 #include "launch.h"
+#include "tiles.h"
 
 using namespace lbman;
 
@@ -167,8 +168,6 @@ int check_launch(lbman_solver* s, cudaError_t e, const char* what) {
     return LBMAN_OK;
 }
 
-// Compiled tile shapes of the z-marching kernels (cells per x-y plane).
-constexpr int kTiles[][2] = {{30, 6}, {32, 6}, {14, 14}, {30, 14}, {62, 6}};
 
 // z chunk giving several waves of blocks over the SMs.
 int default_zchunk(int nx, int ny, int nz, int tcx, int tcy, int num_sms) {
@@ -193,7 +192,7 @@ LaunchShape default_shape(const lbman_config& c, int num_sms, const Ops& ops) {
         int best_wide = -1;
         L.tile.tcx = 30;
         L.tile.tcy = 6;
-        for (const auto& t : kTiles) {
+        for (const auto& t : kTileList) {
             QTile q{t[0], t[1], 1};
             if (ops.qforce_smem(q) == 0) continue;  // not compiled for this precision
             const double padx = (double)((c.nx + t[0] - 1) / t[0] * t[0]) / c.nx;
@@ -647,7 +646,7 @@ int lbman_autotune(lbman_solver* s, int steps_per_trial, lbman_shape* best, int*
         status = fail(LBMAN_ERR_CUDA, "autotune set-up failed");
     } else {
         for (int k : {LBMAN_KERNELS_SPLIT, LBMAN_KERNELS_FUSED}) {
-            for (const auto& t : kTiles) {
+            for (const auto& t : kTileList) {
                 QTile q{t[0], t[1], 1};
                 if (s->ops().qforce_smem(q) == 0) continue;
                 const int z0 = default_zchunk(s->P.nx, s->P.ny, s->P.nz, t[0], t[1], s->num_sms);

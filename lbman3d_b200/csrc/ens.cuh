@@ -36,7 +36,7 @@ struct EnsLbmWork {
 };
 
 template <class TL, class R, bool UPWIND>
-__global__ void __launch_bounds__(TL::NT) ens_qforce_kernel(const EnsBox* __restrict__ boxes,
+__global__ void __launch_bounds__(TL::NT, (Stage<TL, R>::MINB)) ens_qforce_kernel(const EnsBox* __restrict__ boxes,
                                                             const EnsQWork* __restrict__ work, int nwork,
                                                             int par) {
     extern __shared__ __align__(16) unsigned char smem_raw[];

@@ -12,6 +12,7 @@
 #include "../../include/lbman3d.h"
 #include "ens_launch.h"
 #include "launch.h"
+#include "tiles.h"
 
 namespace lbman {
 void set_last_error(const char* msg);
@@ -60,7 +61,6 @@ struct PrecOps {
     }
 const PrecOps kEnsOps[3] = {ENS_OPS(f64), ENS_OPS(f32), ENS_OPS(f16)};
 
-constexpr int kEnsTiles[][2] = {{30, 6}, {32, 6}, {14, 14}, {30, 14}, {62, 6}};
 
 }  // namespace
 
@@ -494,7 +494,7 @@ int lbman_ensemble_autotune(lbman_ensemble* e, int steps_per_trial, lbman_shape*
     lbman_shape win{kern0, tx0, ty0, zc0, 0, 1e30};
     int count = 0, status = LBMAN_OK;
     for (int k : {LBMAN_KERNELS_SPLIT, LBMAN_KERNELS_FUSED}) {
-        for (const auto& t : kEnsTiles) {
+        for (const auto& t : kTileList) {
             if (e->ops().qforce_smem(QTile{t[0], t[1], 1}) == 0) continue;
             for (int zc : {0, 16, 48}) {
                 if ((status = lbman_ensemble_set_shape(e, k, t[0], t[1], zc)) != LBMAN_OK) break;

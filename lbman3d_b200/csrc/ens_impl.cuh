@@ -52,7 +52,8 @@ struct EnsImpl {
 
     static cudaError_t prepare(size_t max_smem) {
         cudaError_t e = cudaSuccess;
-        for (auto [x, y] : {std::pair<int, int>{30, 6}, {32, 6}, {14, 14}, {30, 14}, {62, 6}}) {
+        for (const auto& xy : kTileList) {
+            const int x = xy[0], y = xy[1];
             impl::with_tile<R>(x, y, [&](auto tl) {
                 using TL = decltype(tl);
                 auto attr = [&](auto kern) {

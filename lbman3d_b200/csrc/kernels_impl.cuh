@@ -6,6 +6,7 @@
 #include "init.cuh"
 #include "launch.h"
 #include "reduce.cuh"
+#include "tiles.h"
 
 #include <utility>
 
@@ -33,11 +34,7 @@ cudaError_t with_tile(int tcx, int tcy, F&& f) {
         else                                                               \
             return cudaErrorInvalidValue;                                  \
     }
-    LBMAN_TILE(30, 6)
-    LBMAN_TILE(32, 6)
-    LBMAN_TILE(14, 14)
-    LBMAN_TILE(30, 14)
-    LBMAN_TILE(62, 6)
+    LBMAN_TILES(LBMAN_TILE)
 #undef LBMAN_TILE
     return cudaErrorInvalidValue;
 }
@@ -203,7 +200,8 @@ cudaError_t prepare(size_t max_smem) {
     auto attr = [&](auto kern) {
         if (e == cudaSuccess) e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, b);
     };
-    for (auto [x, y] : {std::pair<int, int>{30, 6}, {32, 6}, {14, 14}, {30, 14}, {62, 6}}) {
+    for (const auto& xy : kTileList) {
+        const int x = xy[0], y = xy[1];
         with_tile<R>(x, y, [&](auto tl) {
             using TL = decltype(tl);
             attr(qforce_kernel<TL, R, true>);

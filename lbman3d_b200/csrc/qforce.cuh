@@ -30,14 +30,41 @@ template <int TCX_, int TCY_>
 struct Tile {
     static constexpr int TCX = TCX_, TCY = TCY_;
     static constexpr int BX = TCX + 2, BY = TCY + 2, NB = BX * BY;  // halo-1 result region
-    static constexpr int UX = TCX + 4, UY = TCY + 4, NQU = UX * UY;  // halo-2 staged region
+    static constexpr int UY = TCY + 4;                               // staged rows (halo 2)
     static constexpr int NT = (NB + 31) / 32 * 32;                   // threads per block
-    static constexpr int NBV = 13;                                   // Q_new 5, Sigma 5, tau 3
     template <class R>
-    static constexpr size_t smem_bytes() {
-        return sizeof(R) * (size_t)(4 * 8 * NQU + 3 * NBV * NB);
-    }
+    static constexpr size_t smem_bytes();
 };
+
+// Shared-memory layout of one block for compute type R.
+//   Staged Q/u: 4 planes x 8 variables x UY rows x UX columns.  FP32 tiles
+//   whose width is a multiple of 4 stage x in [x0-4, x0+TCX+4) as 16-byte
+//   chunks; otherwise x in [x0-2, x0+TCX+2) one value per copy.
+//   Results: FP64 keeps Q_new, Sigma and tau (13 values) for 3 planes and
+//   differentiates each along every axis, in the reference's order.  FP32
+//   keeps the row stress Pi = Sigma + tau - ALPHA Q_new pre-combined per
+//   differentiation axis: 6 values (the x- and y-differenced rows) for the
+//   current and next plane, 3 values (the z-differenced row) for 3 planes.
+template <class TL, class R>
+struct Stage {
+    static constexpr bool VEC = sizeof(R) == 4 && TL::TCX % 4 == 0;
+    static constexpr bool COMB = sizeof(R) == 4;
+    static constexpr int XO = VEC ? 4 : 2;        // staged column of global x0
+    static constexpr int UX = TL::TCX + 2 * XO;   // staged row length
+    static constexpr int NQU = UX * TL::UY;       // one variable of one plane
+    static constexpr int NRES = COMB ? (2 * 6 + 3 * 3) : 3 * 13;
+    static constexpr size_t bytes = sizeof(R) * (size_t)(4 * 8 * NQU + NRES * TL::NB);
+    // Blocks per SM that the shared memory admits (228 KB per SM, 1 KB
+    // reserved per block); the Q+force kernel caps its registers to match.
+    static constexpr int FIT = (int)((228 * 1024) / (bytes + 1024));
+    static constexpr int MINB = FIT < 1 ? 1 : (FIT > 4 ? 4 : FIT);
+};
+
+template <int TCX_, int TCY_>
+template <class R>
+constexpr size_t Tile<TCX_, TCY_>::smem_bytes() {
+    return Stage<Tile<TCX_, TCY_>, R>::bytes;
+}
 
 __device__ __forceinline__ int ring3(int z, int z0) { return (z - z0 + 6) % 3; }
 __device__ __forceinline__ int ring4(int z, int z0) { return (z - z0 + 8) & 3; }
@@ -51,27 +78,51 @@ __device__ __forceinline__ void cp_async(double* s, const double* g) {
     asm volatile("cp.async.ca.shared.global [%0], [%1], 8;\n" ::"r"((unsigned)__cvta_generic_to_shared(s)),
                  "l"(g));
 }
+__device__ __forceinline__ void cp_async16(float* s, const float* g) {
+    asm volatile("cp.async.cg.shared.global [%0], [%1], 16;\n" ::"r"((unsigned)__cvta_generic_to_shared(s)),
+                 "l"(g));
+}
 __device__ __forceinline__ void cp_async_wait_all() { asm volatile("cp.async.wait_all;\n" ::: "memory"); }
 
 // Issue the copies of plane zg (Q then u, tile + 2-cell halo, periodic wrap)
-// into its ring slot; complete at the next cp_async_wait_all().
+// into its ring slot; complete at the next cp_async_wait_all().  vec: 16-byte
+// chunks (FP32, nx a multiple of 4, 16-byte aligned fields), so no chunk
+// straddles the periodic seam.
 template <class TL, class R>
 __device__ __forceinline__ void qf_load_plane(const SimParams& P, int x0, int y0, int z0, int zg,
-                                              const R* __restrict__ qin, const R* __restrict__ uin, R* QU) {
+                                              const R* __restrict__ qin, const R* __restrict__ uin, R* QU,
+                                              bool vec) {
+    using ST = Stage<TL, R>;
     const int zw = wrap_coord(zg, P.nz);
-    R* dst = QU + ring4(zg, z0) * 8 * TL::NQU;
-    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
-    constexpr int nwarp = TL::NT / 32;
+    R* dst = QU + ring4(zg, z0) * 8 * ST::NQU;
     const int64_t zoff = (int64_t)zw * P.nxy;
+    if constexpr (ST::VEC) {
+        if (vec) {
+            constexpr int CH = ST::UX / 4;
+            constexpr int N = 8 * TL::UY * CH;
 #pragma unroll 1
-    for (int row = warp; row < 8 * TL::UY; row += nwarp) {
+            for (int i = threadIdx.x; i < N; i += TL::NT) {
+                const int row = i / CH, ch = i - row * CH;
+                const int var = row / TL::UY, ly = row - var * TL::UY;
+                const int gy = wrap_coord(y0 - 2 + ly, P.ny);
+                const int gx = wrap_coord(x0 - ST::XO + 4 * ch, P.nx);
+                const R* src = (var < 5 ? qin + (int64_t)var * P.V : uin + (int64_t)(var - 5) * P.V) + zoff +
+                               (int64_t)gy * P.nx + gx;
+                cp_async16(dst + var * ST::NQU + ly * ST::UX + 4 * ch, src);
+            }
+            return;
+        }
+    }
+    constexpr int N = 8 * TL::UY * ST::UX;
+#pragma unroll 1
+    for (int i = threadIdx.x; i < N; i += TL::NT) {
+        const int row = i / ST::UX, lx = i - row * ST::UX;
         const int var = row / TL::UY, ly = row - var * TL::UY;
         const int gy = wrap_coord(y0 - 2 + ly, P.ny);
+        const int gx = wrap_coord(x0 - ST::XO + lx, P.nx);
         const R* src = (var < 5 ? qin + (int64_t)var * P.V : uin + (int64_t)(var - 5) * P.V) + zoff +
-                       (int64_t)gy * P.nx;
-        R* d = dst + var * TL::NQU + ly * TL::UX;
-#pragma unroll
-        for (int lx = lane; lx < TL::UX; lx += 32) cp_async(d + lx, src + wrap_coord(x0 - 2 + lx, P.nx));
+                       (int64_t)gy * P.nx + gx;
+        cp_async(dst + var * ST::NQU + ly * ST::UX + lx, src);
     }
 }
 
@@ -104,18 +155,19 @@ __device__ __forceinline__ PointGeo point_geo(const SimParams& P, int x0, int y0
 }
 
 // Beris-Edwards update of this thread's point in plane zb; results to the
-// ring slot of zb, Ericksen force to er.
+// ring slots of zb, Ericksen force to er, Q_new to qn.
 template <class TL, class R, bool UPWIND>
 __device__ __forceinline__ void qf_compute_plane(const SimParams& P, const Phys<R>& K, const PointGeo& G,
                                                  const AxisRule& qx, const AxisRule& qy, const VRule& vx,
                                                  const VRule& vy, int z0, int zb, const R* QU, R* Bs,
-                                                 R er[3]) {
+                                                 R er[3], R qn[5]) {
     if (!G.hasB) return;
-    constexpr int NQU = TL::NQU, UX = TL::UX, NB = TL::NB;
+    using ST = Stage<TL, R>;
+    constexpr int NQU = ST::NQU, UX = ST::UX, NB = TL::NB;
     const R* Qc = QU + ring4(zb, z0) * 8 * NQU;
     const R* Qm = QU + ring4(zb - 1, z0) * 8 * NQU;
     const R* Qp = QU + ring4(zb + 1, z0) * 8 * NQU;
-    const int up = (G.lby + 1) * UX + G.lbx + 1;
+    const int up = (G.lby + 1) * UX + G.lbx + ST::XO - 1;
     AxisRule qz;
     VRule vz;
     if (G.wz) {
@@ -157,72 +209,154 @@ __device__ __forceinline__ void qf_compute_plane(const SimParams& P, const Phys<
     g.ux_x = gr[0]; g.ux_y = gr[1]; g.ux_z = gr[2];
     g.uy_x = gr[3]; g.uy_y = gr[4]; g.uy_z = gr[5];
     g.uz_x = gr[6]; g.uz_y = gr[7];
-    R qn[5], sg[5], ta[3];
+    R sg[5], ta[3];
     pointwise_q<R, UPWIND>(K, Q, u0[0], u0[1], u0[2], d, g, qn, sg, ta, er);
-    R* Bd = Bs + ring3(zb, z0) * TL::NBV * NB + threadIdx.x;
+    if constexpr (ST::COMB) {
+        // Row stress Pi_ab = Sigma_ab + tau_ab - ALPHA Q_new_ab (tau_ba = -tau_ab),
+        // grouped by the axis b it is differentiated along (f_a = d_b Pi_ab).
+        const R a = -K.ALPHA;
+        R* Bxy = Bs + ((zb - z0) & 1) * 6 * NB + threadIdx.x;
+        R* Bz = Bs + 12 * NB + ring3(zb, z0) * 3 * NB + threadIdx.x;
+        Bxy[0 * NB] = sg[0] + a * qn[0];
+        Bxy[1 * NB] = (sg[1] - ta[0]) + a * qn[1];
+        Bxy[2 * NB] = (sg[2] - ta[1]) + a * qn[2];
+        Bxy[3 * NB] = (sg[1] + ta[0]) + a * qn[1];
+        Bxy[4 * NB] = sg[3] + a * qn[3];
+        Bxy[5 * NB] = (sg[4] - ta[2]) + a * qn[4];
+        Bz[0 * NB] = (sg[2] + ta[1]) + a * qn[2];
+        Bz[1 * NB] = (sg[4] + ta[2]) + a * qn[4];
+        Bz[2 * NB] = -(sg[0] + sg[3]) - a * (qn[0] + qn[3]);
+    } else {
+        R* Bd = Bs + ring3(zb, z0) * 13 * NB + threadIdx.x;
 #pragma unroll
-    for (int k = 0; k < 5; ++k) Bd[k * NB] = qn[k];
+        for (int k = 0; k < 5; ++k) Bd[k * NB] = qn[k];
 #pragma unroll
-    for (int k = 0; k < 5; ++k) Bd[(5 + k) * NB] = sg[k];
+        for (int k = 0; k < 5; ++k) Bd[(5 + k) * NB] = sg[k];
 #pragma unroll
-    for (int k = 0; k < 3; ++k) Bd[(10 + k) * NB] = ta[k];
+        for (int k = 0; k < 3; ++k) Bd[(10 + k) * NB] = ta[k];
+    }
+}
+
+// Difference of the active term's Q_new derivative between the anchoring
+// ghost and the index clamp, at a wall cell: the clamp takes the centre c
+// for the missing neighbour, the ghost 2A - c (QAxisGhostPair,
+// src/boundary_handler.h:253-282), so d_ghost - d_clamp = c - A_lo at the
+// low face and A_hi - c at the high face.
+template <class R>
+__device__ __forceinline__ R anchor_delta(const AxisRule& r, const Phys<R>& K, int k, R c) {
+    R d = R(0);
+    if (r.m_ghost) d += c - K.anchor[r.lo][k];
+    if (r.p_ghost) d += K.anchor[r.hi][k] - c;
+    return d;
 }
 
 // Body force of this thread's tile cell in plane zc from the staged result
-// planes; out(cell, x, y, z, qn[5], F[3], u[3]) consumes it.
+// planes; out(cell, x, y, z, qn[5], F[3], u[3]) consumes it.  qc is the
+// cell's Q_new (kept in registers by the FP32 path).
 template <class TL, class R, class OutFn>
 __device__ __forceinline__ void qf_force_cell(const SimParams& P, const Phys<R>& K, const PointGeo& G,
                                               const AxisRule& qx, const AxisRule& qy, int x0, int y0, int z0,
-                                              int zc, const R* QU, const R* Bs, const R er[3], OutFn&& out) {
+                                              int zc, const R* QU, const R* Bs, const R er[3], const R qc[5],
+                                              OutFn&& out) {
     if (!G.isC) return;
-    constexpr int NB = TL::NB, BX = TL::BX, NBV = TL::NBV;
+    using ST = Stage<TL, R>;
+    constexpr int NB = TL::NB, BX = TL::BX;
     const int t = threadIdx.x;
-    const R* B0 = Bs + ring3(zc, z0) * NBV * NB;
-    const R* Bm = Bs + ring3(zc - 1, z0) * NBV * NB;
-    const R* Bp = Bs + ring3(zc + 1, z0) * NBV * NB;
     const int gx = x0 + G.lbx - 1, gy = y0 + G.lby - 1;
     AxisRule qz;
     if (G.wz) qz = q_rule(P, 2, zc, P.nz);
-    // grad Q_new with the wall ghosts (QGradientAndLaplacian on the new Q)
-    R dQ[5][3], qn[5];
-#pragma unroll
-    for (int k = 0; k < 5; ++k) {
-        const R* b = B0 + k * NB;
-        const R c = b[t];
-        qn[k] = c;
-        R xm = b[t - 1], xp = b[t + 1], ym = b[t - BX], yp = b[t + BX];
-        R zm = Bm[k * NB + t], zp = Bp[k * NB + t];
-        if (G.wx) q_apply<R>(qx, K, k, c, xm, xp);
-        if (G.wy) q_apply<R>(qy, K, k, c, ym, yp);
-        if (G.wz) q_apply<R>(qz, K, k, c, zm, zp);
-        dQ[k][0] = R(0.5) * (xp - xm);
-        dQ[k][1] = R(0.5) * (yp - ym);
-        dQ[k][2] = R(0.5) * (zp - zm);
-    }
     // Sigma / tau differences with the Neumann/periodic index clamp QXoff
     // (src/offsets.h:59-83, used by PassiveStressDivergence).
     const bool xmc = G.wx && gx == 0 && !P.qper[0], xpc = G.wx && gx == P.nx - 1 && !P.qper[1];
     const bool ymc = G.wy && gy == 0 && !P.qper[2], ypc = G.wy && gy == P.ny - 1 && !P.qper[3];
     const bool zmc = G.wz && zc == 0 && !P.qper[4], zpc = G.wz && zc == P.nz - 1 && !P.qper[5];
-    R dS[3][5], dT[3][3];
-#pragma unroll
-    for (int v = 0; v < 8; ++v) {
-        const R* b = B0 + (5 + v) * NB;
-        const R c = b[t];
-        const R xm = xmc ? c : b[t - 1], xp = xpc ? c : b[t + 1];
-        const R ym = ymc ? c : b[t - BX], yp = ypc ? c : b[t + BX];
-        const R zm = zmc ? c : Bm[(5 + v) * NB + t], zp = zpc ? c : Bp[(5 + v) * NB + t];
-        const R ddx = R(0.5) * (xp - xm), ddy = R(0.5) * (yp - ym), ddz = R(0.5) * (zp - zm);
-        if (v < 5) { dS[0][v] = ddx; dS[1][v] = ddy; dS[2][v] = ddz; }
-        else { dT[0][v - 5] = ddx; dT[1][v - 5] = ddy; dT[2][v - 5] = ddz; }
-    }
-    const R* U0 = QU + ring4(zc, z0) * 8 * TL::NQU;
-    const int up = (G.lby + 1) * TL::UX + G.lbx + 1;
-    const R u[3] = {U0[5 * TL::NQU + up], U0[6 * TL::NQU + up], U0[7 * TL::NQU + up]};
+    const R* U0 = QU + ring4(zc, z0) * 8 * ST::NQU;
+    const int up = (G.lby + 1) * ST::UX + G.lbx + ST::XO - 1;
+    const R u[3] = {U0[5 * ST::NQU + up], U0[6 * ST::NQU + up], U0[7 * ST::NQU + up]};
     R F[3];
-    active_passive_force<R>(K, dQ, dS, dT, u[0], u[1], u[2], er, F);
-    const int64_t cell = (int64_t)zc * P.nxy + (int64_t)gy * P.nx + gx;
-    out(cell, gx, gy, zc, qn, F, u);
+    if constexpr (ST::COMB) {
+        const R* Bxy = Bs + ((zc - z0) & 1) * 6 * NB + t;
+        const R* Bz = Bs + 12 * NB + t;
+        const R* Bzm = Bz + ring3(zc - 1, z0) * 3 * NB;
+        const R* Bzp = Bz + ring3(zc + 1, z0) * 3 * NB;
+        const R* Bz0 = Bz + ring3(zc, z0) * 3 * NB;
+        R f[3];
+#pragma unroll
+        for (int a = 0; a < 3; ++a) {
+            const R* px = Bxy + a * NB;
+            const R* py = Bxy + (3 + a) * NB;
+            R xm = px[-1], xp = px[1], ym = py[-BX], yp = py[BX];
+            R zm = Bzm[a * NB], zp = Bzp[a * NB];
+            if (G.wx) {
+                if (xmc) xm = px[0];
+                if (xpc) xp = px[0];
+            }
+            if (G.wy) {
+                if (ymc) ym = py[0];
+                if (ypc) yp = py[0];
+            }
+            if (G.wz) {
+                if (zmc) zm = Bz0[a * NB];
+                if (zpc) zp = Bz0[a * NB];
+            }
+            f[a] = R(0.5) * (xp - xm) + R(0.5) * (yp - ym) + R(0.5) * (zp - zm);
+        }
+        if (G.wx && (qx.m_ghost || qx.p_ghost)) {
+            f[0] += -K.ALPHA * anchor_delta<R>(qx, K, 0, qc[0]);
+            f[1] += -K.ALPHA * anchor_delta<R>(qx, K, 1, qc[1]);
+            f[2] += -K.ALPHA * anchor_delta<R>(qx, K, 2, qc[2]);
+        }
+        if (G.wy && (qy.m_ghost || qy.p_ghost)) {
+            f[0] += -K.ALPHA * anchor_delta<R>(qy, K, 1, qc[1]);
+            f[1] += -K.ALPHA * anchor_delta<R>(qy, K, 3, qc[3]);
+            f[2] += -K.ALPHA * anchor_delta<R>(qy, K, 4, qc[4]);
+        }
+        if (G.wz && (qz.m_ghost || qz.p_ghost)) {
+            f[0] += -K.ALPHA * anchor_delta<R>(qz, K, 2, qc[2]);
+            f[1] += -K.ALPHA * anchor_delta<R>(qz, K, 4, qc[4]);
+            f[2] += K.ALPHA * (anchor_delta<R>(qz, K, 0, qc[0]) + anchor_delta<R>(qz, K, 3, qc[3]));
+        }
+        F[0] = er[0] + (f[0] - K.MU * u[0]);
+        F[1] = er[1] + (f[1] - K.MU * u[1]);
+        F[2] = er[2] + (f[2] - K.MU * u[2]);
+        const int64_t cell = (int64_t)zc * P.nxy + (int64_t)gy * P.nx + gx;
+        out(cell, gx, gy, zc, qc, F, u);
+    } else {
+        const R* B0 = Bs + ring3(zc, z0) * 13 * NB;
+        const R* Bm = Bs + ring3(zc - 1, z0) * 13 * NB;
+        const R* Bp = Bs + ring3(zc + 1, z0) * 13 * NB;
+        // grad Q_new with the wall ghosts (QGradientAndLaplacian on the new Q)
+        R dQ[5][3], qn[5];
+#pragma unroll
+        for (int k = 0; k < 5; ++k) {
+            const R* b = B0 + k * NB;
+            const R c = b[t];
+            qn[k] = c;
+            R xm = b[t - 1], xp = b[t + 1], ym = b[t - BX], yp = b[t + BX];
+            R zm = Bm[k * NB + t], zp = Bp[k * NB + t];
+            if (G.wx) q_apply<R>(qx, K, k, c, xm, xp);
+            if (G.wy) q_apply<R>(qy, K, k, c, ym, yp);
+            if (G.wz) q_apply<R>(qz, K, k, c, zm, zp);
+            dQ[k][0] = R(0.5) * (xp - xm);
+            dQ[k][1] = R(0.5) * (yp - ym);
+            dQ[k][2] = R(0.5) * (zp - zm);
+        }
+        R dS[3][5], dT[3][3];
+#pragma unroll
+        for (int v = 0; v < 8; ++v) {
+            const R* b = B0 + (5 + v) * NB;
+            const R c = b[t];
+            const R xm = xmc ? c : b[t - 1], xp = xpc ? c : b[t + 1];
+            const R ym = ymc ? c : b[t - BX], yp = ypc ? c : b[t + BX];
+            const R zm = zmc ? c : Bm[(5 + v) * NB + t], zp = zpc ? c : Bp[(5 + v) * NB + t];
+            const R ddx = R(0.5) * (xp - xm), ddy = R(0.5) * (yp - ym), ddz = R(0.5) * (zp - zm);
+            if (v < 5) { dS[0][v] = ddx; dS[1][v] = ddy; dS[2][v] = ddz; }
+            else { dT[0][v - 5] = ddx; dT[1][v - 5] = ddy; dT[2][v - 5] = ddz; }
+        }
+        active_passive_force<R>(K, dQ, dS, dT, u[0], u[1], u[2], er, F);
+        const int64_t cell = (int64_t)zc * P.nxy + (int64_t)gy * P.nx + gx;
+        out(cell, gx, gy, zc, qn, F, u);
+    }
 }
 
 // Marches a block through its z chunk.  The copy of plane zc+3 is in flight
@@ -231,8 +365,9 @@ template <class TL, class R, bool UPWIND, class OutFn>
 __device__ __forceinline__ void qf_march(const SimParams& P, int zc_len, const R* __restrict__ qin,
                                          const R* __restrict__ uin, R* smem, OutFn&& out, int bx, int by,
                                          int bz) {
+    using ST = Stage<TL, R>;
     R* QU = smem;
-    R* Bs = smem + 4 * 8 * TL::NQU;
+    R* Bs = smem + 4 * 8 * ST::NQU;
     const int x0 = bx * TL::TCX, y0 = by * TL::TCY;
     const int z0 = bz * zc_len;
     if (z0 >= P.nz) return;
@@ -241,25 +376,29 @@ __device__ __forceinline__ void qf_march(const SimParams& P, int zc_len, const R
     const PointGeo G = point_geo<TL>(P, x0, y0, z0, z1);
     const AxisRule qx = q_rule(P, 0, G.ax, P.nx), qy = q_rule(P, 1, G.ay, P.ny);
     const VRule vx = v_rule(P, 0, G.ax, P.nx), vy = v_rule(P, 1, G.ay, P.ny);
-    R er_cur[3], er_next[3];
+    const bool vec = ST::VEC && (P.nx & 3) == 0 &&
+                     ((reinterpret_cast<uintptr_t>(qin) | reinterpret_cast<uintptr_t>(uin)) & 15) == 0;
+    R er_cur[3], er_next[3], qn_cur[5], qn_next[5];
 
-    for (int z = z0 - 2; z <= z0 + 1; ++z) qf_load_plane<TL>(P, x0, y0, z0, z, qin, uin, QU);
+    for (int z = z0 - 2; z <= z0 + 1; ++z) qf_load_plane<TL>(P, x0, y0, z0, z, qin, uin, QU, vec);
     cp_async_wait_all();
     __syncthreads();
-    qf_compute_plane<TL, R, UPWIND>(P, K, G, qx, qy, vx, vy, z0, z0 - 1, QU, Bs, er_next);
-    qf_compute_plane<TL, R, UPWIND>(P, K, G, qx, qy, vx, vy, z0, z0, QU, Bs, er_cur);
+    qf_compute_plane<TL, R, UPWIND>(P, K, G, qx, qy, vx, vy, z0, z0 - 1, QU, Bs, er_next, qn_next);
+    qf_compute_plane<TL, R, UPWIND>(P, K, G, qx, qy, vx, vy, z0, z0, QU, Bs, er_cur, qn_cur);
     __syncthreads();  // the slot of z0-2 is free again
-    qf_load_plane<TL>(P, x0, y0, z0, z0 + 2, qin, uin, QU);
+    qf_load_plane<TL>(P, x0, y0, z0, z0 + 2, qin, uin, QU, vec);
     cp_async_wait_all();
     __syncthreads();
 #pragma unroll 1
     for (int zc = z0; zc < z1; ++zc) {
-        if (zc + 1 < z1) qf_load_plane<TL>(P, x0, y0, z0, zc + 3, qin, uin, QU);
-        qf_compute_plane<TL, R, UPWIND>(P, K, G, qx, qy, vx, vy, z0, zc + 1, QU, Bs, er_next);
+        if (zc + 1 < z1) qf_load_plane<TL>(P, x0, y0, z0, zc + 3, qin, uin, QU, vec);
+        qf_compute_plane<TL, R, UPWIND>(P, K, G, qx, qy, vx, vy, z0, zc + 1, QU, Bs, er_next, qn_next);
         __syncthreads();
-        qf_force_cell<TL, R>(P, K, G, qx, qy, x0, y0, z0, zc, QU, Bs, er_cur, out);
+        qf_force_cell<TL, R>(P, K, G, qx, qy, x0, y0, z0, zc, QU, Bs, er_cur, qn_cur, out);
 #pragma unroll
         for (int k = 0; k < 3; ++k) er_cur[k] = er_next[k];
+#pragma unroll
+        for (int k = 0; k < 5; ++k) qn_cur[k] = qn_next[k];
         cp_async_wait_all();
         __syncthreads();
     }
@@ -281,7 +420,7 @@ struct StoreQForce {
 };
 
 template <class TL, class R, bool UPWIND>
-__global__ void __launch_bounds__(TL::NT) qforce_kernel(const __grid_constant__ SimParams P, int zc_len,
+__global__ void __launch_bounds__(TL::NT, (Stage<TL, R>::MINB)) qforce_kernel(const __grid_constant__ SimParams P, int zc_len,
                                                         const R* __restrict__ qin, const R* __restrict__ uin,
                                                         R* __restrict__ qout, R* __restrict__ Fout) {
     extern __shared__ __align__(16) unsigned char smem_raw[];

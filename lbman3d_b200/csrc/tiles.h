@@ -1,0 +1,13 @@
+// tiles.h -- the compiled z-marching tile shapes (cells per x-y plane of one
+// block) of the Q+force, fused and ensemble kernels.  A shape whose shared
+// memory does not fit one block for a precision is skipped for it.
+#pragma once
+
+#define LBMAN_TILES(X) X(30, 6) X(32, 6) X(14, 14) X(30, 14) X(62, 6) X(32, 8) X(32, 14) X(64, 6)
+
+namespace lbman {
+#define LBMAN_TILE_PAIR(x, y) {x, y},
+constexpr int kTileList[][2] = {LBMAN_TILES(LBMAN_TILE_PAIR)};
+#undef LBMAN_TILE_PAIR
+constexpr int kNumTiles = sizeof(kTileList) / sizeof(kTileList[0]);
+}  // namespace lbman
