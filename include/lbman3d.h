@@ -186,14 +186,20 @@ int lbman_flow_reduce_noalloc(int64_t ncells, int precision, const void* rho, co
 typedef struct lbman_shape {
     int kernels;              /* LBMAN_KERNELS_SPLIT / LBMAN_KERNELS_FUSED     */
     int tile_x, tile_y;       /* cells per x-y plane of one block             */
-    int zchunk;               /* z planes marched by one block                */
+    int zchunk;               /* > 0: z planes marched by one block;
+                                 <= 0: balanced schedule, max(1, -zchunk)
+                                 waves of resident blocks, each taking an
+                                 equal share of the column planes            */
     int threads;              /* threads per block (set by the tile)          */
     double ms_per_step;       /* measured by lbman_autotune, else 0           */
+    int blocks;               /* blocks of the Q+force (or fused) launch of a
+                                 solver; 0 from the ensemble calls           */
 } lbman_shape;
 
 int lbman_get_shape(lbman_solver* s, lbman_shape* out);
 /* Select a shape (tile_x x tile_y must be one of the compiled tiles: 30x6,
- * 32x6, 14x14, and for FP32/FP16 also 30x14, 62x6; zchunk >= 1).           */
+ * 32x6, 14x14, 32x8, and for FP32/FP16 also 30x14, 62x6, 32x14, 64x6;
+ * zchunk >= -8).                                                           */
 int lbman_set_shape(lbman_solver* s, const lbman_shape* shape);
 /* Autotuner (no counterpart in the reference): times steps_per_trial steps
  * of every kernel organisation x compiled tile x z-chunk candidate on the
@@ -230,6 +236,38 @@ int lbman_ensemble_get_shape(lbman_ensemble* e, lbman_shape* out);
  * ensemble, keeps the fastest, restores every box's state bit for bit.     */
 int lbman_ensemble_autotune(lbman_ensemble* e, int steps_per_trial, lbman_shape* best, int* ntrials);
 int lbman_ensemble_info(lbman_ensemble* e, int64_t* cells, int64_t* steps, int64_t* launches);
+
+/* Statistics of the current state (no counterpart in the reference, whose
+ * analysis stops at the defect finder).  The first call allocates cuFFT
+ * plans and scratch (about 5 x 8 x V bytes in FP64, half that otherwise),
+ * kept until lbman_destroy.  Every axis is transformed as periodic.  Shell
+ * sums are accumulated in FP64; 1 <= nbins <= 8192; shells beyond nbins are
+ * dropped.                                                                  */
+#define LBMAN_STATS_MAX_BINS 8192
+
+/* Shell-averaged kinetic-energy spectrum: E[b] = (1 / 2V^2) sum of |u_hat(k)|^2
+ * over the wavevectors of shell b = round(n_max |(m_x/nx, m_y/ny, m_z/nz)|),
+ * m the integer wavenumbers (|m_a| <= n_a/2), n_max = max(nx, ny, nz);
+ * sum_b E[b] = <|u|^2>/2 once nbins > n_max*sqrt(3)/2.  counts (may be NULL)
+ * receives the number of wavevectors per shell.                            */
+int lbman_velocity_spectrum(lbman_solver* s, int nbins, double* E, double* counts);
+
+/* Radially averaged Q-tensor autocorrelation C[b] = <Q(x):Q(x+r)> / <Q:Q>
+ * (full 3x3 contraction, qzz = -qxx - qyy), r binned by b = round(|r|) with
+ * minimum-image separations; counts (may be NULL) receives the separations
+ * per shell.  xi (may be NULL) receives the correlation length: the |r| at
+ * which C first falls below 1/e, linearly interpolated between shells, or
+ * -1 if it does not within nbins shells.                                    */
+int lbman_q_correlation(lbman_solver* s, int nbins, double* C, double* counts, double* xi);
+
+typedef struct lbman_stats {
+    double mean_speed;        /* <|u|> over cells                              */
+    double rms_speed;         /* sqrt(<|u|^2>)                                  */
+    int64_t defect_faces;     /* as lbman_reduce(LBMAN_DIAG_DEFECTS), -1 if any
+                                 side is below 2 cells                          */
+    double defect_density;    /* defect_faces / V, -1 if not computed          */
+} lbman_stats;
+int lbman_statistics(lbman_solver* s, lbman_stats* out);
 
 /* Steps completed since the last upload. */
 int lbman_steps_done(lbman_solver* s, int64_t* steps);

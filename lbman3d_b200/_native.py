@@ -44,7 +44,15 @@ class lbman_diag(C.Structure):
 
 class lbman_shape(C.Structure):
     _fields_ = [("kernels", C.c_int), ("tile_x", C.c_int), ("tile_y", C.c_int), ("zchunk", C.c_int),
-                ("threads", C.c_int), ("ms_per_step", C.c_double)]
+                ("threads", C.c_int), ("ms_per_step", C.c_double), ("blocks", C.c_int)]
+
+
+class lbman_stats(C.Structure):
+    _fields_ = [("mean_speed", C.c_double), ("rms_speed", C.c_double), ("defect_faces", C.c_int64),
+                ("defect_density", C.c_double)]
+
+
+STATS_MAX_BINS = 8192
 
 
 class LbmanError(RuntimeError):
@@ -98,6 +106,9 @@ PROTOTYPES = [
     ("lbman_ensemble_autotune", C.c_int, [C.c_void_p, C.c_int, C.POINTER(lbman_shape), C.POINTER(C.c_int)]),
     ("lbman_ensemble_info", C.c_int, [C.c_void_p, C.POINTER(C.c_int64), C.POINTER(C.c_int64),
                                       C.POINTER(C.c_int64)]),
+    ("lbman_velocity_spectrum", C.c_int, [C.c_void_p, C.c_int, _DP, _DP]),
+    ("lbman_q_correlation", C.c_int, [C.c_void_p, C.c_int, _DP, _DP, _DP]),
+    ("lbman_statistics", C.c_int, [C.c_void_p, C.POINTER(lbman_stats)]),
     ("lbman_flow_reduce_noalloc", C.c_int,
      [C.c_int64, C.c_int, C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p, C.POINTER(lbman_diag)]),
 ]

@@ -7,6 +7,9 @@ Translation units and their flags:
   kernels_f32.cu  default contraction (FP32 path)
   kernels_f16.cu  default contraction (FP16 population storage)
   api.cu          host C ABI
+  ens_api.cu      ensemble runner
+  noalloc.cu      allocation-free flow diagnostics
+  stats.cu        spectrum / correlation / speed statistics (links cuFFT)
 Objects go to lbman3d_b200/_build/ (git-ignored).
 """
 from __future__ import annotations
@@ -38,6 +41,7 @@ UNITS = {
     "api.cu": [],
     "ens_api.cu": [],
     "noalloc.cu": [],
+    "stats.cu": [],
 }
 
 
@@ -77,7 +81,7 @@ def build(force: bool = False, verbose: bool = False) -> str:
                     sys.stderr.write(r.stdout + r.stderr)
                     raise RuntimeError("nvcc failed: " + " ".join(cmd))
     if force or jobs or not os.path.exists(LIB):
-        cmd = [NVCC] + ARCH + ["-shared", "-o", LIB] + objs + ["-lcudart"]
+        cmd = [NVCC] + ARCH + ["-shared", "-o", LIB] + objs + ["-lcudart", "-lcufft"]
         if verbose:
             print(" ".join(cmd))
         subprocess.run(cmd, check=True)

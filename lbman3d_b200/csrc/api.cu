@@ -11,6 +11,7 @@
 
 #include "../../include/lbman3d.h"
 #include "launch.h"
+#include "stats.h"
 #include "tiles.h"
 
 using namespace lbman;
@@ -60,6 +61,7 @@ struct Ops {
     decltype(&launch_seeded_init_f64) seeded_init;
     decltype(&qforce_smem_f64) qforce_smem;
     decltype(&qforce_threads_f64) qforce_threads;
+    decltype(&march_blocks_f64) march_blocks;
     decltype(&prepare_f64) prepare;
 };
 
@@ -69,7 +71,7 @@ struct Ops {
             launch_feq_init_##SUF, launch_pop_in_##SUF, launch_pop_out_##SUF, launch_real_in_##SUF,    \
             launch_real_out_##SUF, launch_flow_reduce_##SUF, launch_energy_reduce_##SUF,               \
             launch_director_##SUF, launch_defect_count_##SUF, launch_seeded_init_##SUF,               \
-            qforce_smem_##SUF, qforce_threads_##SUF, prepare_##SUF                                     \
+            qforce_smem_##SUF, qforce_threads_##SUF, march_blocks_##SUF, prepare_##SUF                 \
     }
 
 const Ops kOps[3] = {LBMAN_OPS(f64), LBMAN_OPS(f32), LBMAN_OPS(f16)};
@@ -152,6 +154,7 @@ struct lbman_solver {
     bool own_stream = false;
     int64_t steps = 0, launches = 0;
     int num_sms = 148;
+    lbman::stats::Workspace* stats = nullptr;
     const Ops& ops() const { return kOps[prec]; }
 };
 
@@ -211,7 +214,8 @@ LaunchShape default_shape(const lbman_config& c, int num_sms, const Ops& ops) {
         }
     }
     L.qthreads = ops.qforce_threads(L.tile);
-    L.tile.zc = c.zchunk > 0 ? c.zchunk : default_zchunk(c.nx, c.ny, c.nz, L.tile.tcx, L.tile.tcy, num_sms);
+    L.tile.zc = c.zchunk > 0 ? c.zchunk : 0;  // 0: balanced schedule, one wave
+    L.num_sms = num_sms;
     return L;
 }
 
@@ -395,6 +399,7 @@ int lbman_destroy(lbman_solver* s) {
     for (int b = 0; b < 2; ++b) { cudaFree(s->f[b]); cudaFree(s->q[b]); cudaFree(s->u[b]); }
     cudaFree(s->rho); cudaFree(s->F); cudaFree(s->staging); cudaFree(s->partials); cudaFree(s->red_dev);
     cudaFree(s->upast); cudaFree(s->dirbuf);
+    lbman::stats::destroy(s->stats);
     if (s->red_host) cudaFreeHost(s->red_host);
     if (s->own_stream && s->stream) cudaStreamDestroy(s->stream);
     delete s;
@@ -587,6 +592,68 @@ int lbman_reduce(lbman_solver* s, int flags, lbman_diag* out) {
     return LBMAN_OK;
 }
 
+namespace {
+
+int stats_ready(lbman_solver* s, int nbins) {
+    if (!s->uploaded) return fail(LBMAN_ERR_STATE, "statistics before upload");
+    if (nbins < 1 || nbins > lbman::stats::kMaxBins)
+        return fail(LBMAN_ERR_ARG, "nbins must be in [1, %d]", lbman::stats::kMaxBins);
+    LB_TRY(set_device(s));
+    if (!s->stats) s->stats = lbman::stats::create(s->P.nx, s->P.ny, s->P.nz, s->prec == LBMAN_FP64, s->num_sms);
+    return LBMAN_OK;
+}
+
+int stats_status(int code, const char* what) {
+    if (code == 0) return LBMAN_OK;
+    const int st = lbman::stats::is_nomem(code) ? LBMAN_ERR_NOMEM : LBMAN_ERR_CUDA;
+    return fail(st, "%s: %s", what, lbman::stats::err_string(code));
+}
+
+}  // namespace
+
+int lbman_velocity_spectrum(lbman_solver* s, int nbins, double* E, double* counts) {
+    if (!s || !E) return fail(LBMAN_ERR_ARG, "null argument");
+    LB_TRY(stats_ready(s, nbins));
+    s->launches += 5;  // power x3, shell binning, fold (plus cuFFT's own kernels)
+    return stats_status(lbman::stats::velocity_spectrum(s->stats, s->u[s->ucur], nbins, E, counts, s->stream),
+                        "velocity spectrum");
+}
+
+int lbman_q_correlation(lbman_solver* s, int nbins, double* C, double* counts, double* xi) {
+    if (!s || !C) return fail(LBMAN_ERR_ARG, "null argument");
+    LB_TRY(stats_ready(s, nbins));
+    s->launches += 7;  // power x4, to-complex, shell binning, fold (plus cuFFT's own kernels)
+    LB_TRY(stats_status(lbman::stats::q_correlation(s->stats, s->q[s->qcur], nbins, C, counts, s->stream),
+                        "Q correlation"));
+    if (xi) {
+        *xi = -1.0;
+        const double target = std::exp(-1.0);
+        for (int b = 1; b < nbins; ++b) {
+            if (C[b] < target) {
+                *xi = (b - 1) + (C[b - 1] - target) / (C[b - 1] - C[b]);
+                break;
+            }
+        }
+    }
+    return LBMAN_OK;
+}
+
+int lbman_statistics(lbman_solver* s, lbman_stats* out) {
+    if (!s || !out) return fail(LBMAN_ERR_ARG, "null argument");
+    LB_TRY(stats_ready(s, 2));
+    std::memset(out, 0, sizeof(*out));
+    double m1 = 0.0, m2 = 0.0;
+    s->launches += 2;
+    LB_TRY(stats_status(lbman::stats::speed_moments(s->stats, s->u[s->ucur], &m1, &m2, s->stream), "speed moments"));
+    out->mean_speed = m1;
+    out->rms_speed = std::sqrt(m2);
+    lbman_diag d;
+    LB_TRY(lbman_reduce(s, LBMAN_DIAG_DEFECTS, &d));
+    out->defect_faces = d.defect_faces;
+    out->defect_density = d.defect_faces >= 0 ? (double)d.defect_faces / (double)s->P.V : -1.0;
+    return LBMAN_OK;
+}
+
 int lbman_get_shape(lbman_solver* s, lbman_shape* out) {
     if (!s || !out) return fail(LBMAN_ERR_ARG, "null argument");
     out->kernels = s->kernels;
@@ -595,6 +662,7 @@ int lbman_get_shape(lbman_solver* s, lbman_shape* out) {
     out->zchunk = s->shape.tile.zc;
     out->threads = s->shape.qthreads;
     out->ms_per_step = 0.0;
+    out->blocks = s->ops().march_blocks(s->P, s->shape, s->kernels == LBMAN_KERNELS_FUSED);
     return LBMAN_OK;
 }
 
@@ -603,7 +671,7 @@ int lbman_set_shape(lbman_solver* s, const lbman_shape* sh) {
     if (sh->kernels != LBMAN_KERNELS_SPLIT && sh->kernels != LBMAN_KERNELS_FUSED)
         return fail(LBMAN_ERR_ARG, "kernels must be LBMAN_KERNELS_SPLIT or LBMAN_KERNELS_FUSED");
     QTile t{sh->tile_x, sh->tile_y, sh->zchunk};
-    if (sh->zchunk < 1) return fail(LBMAN_ERR_ARG, "zchunk must be >= 1");
+    if (sh->zchunk < -8) return fail(LBMAN_ERR_ARG, "zchunk must be >= -8 (<= 0: balanced schedule)");
     if (s->ops().qforce_smem(t) == 0)
         return fail(LBMAN_ERR_ARG, "tile %dx%d is not compiled for this precision", sh->tile_x, sh->tile_y);
     s->kernels = sh->kernels;
@@ -649,10 +717,12 @@ int lbman_autotune(lbman_solver* s, int steps_per_trial, lbman_shape* best, int*
             for (const auto& t : kTileList) {
                 QTile q{t[0], t[1], 1};
                 if (s->ops().qforce_smem(q) == 0) continue;
+                // the balanced one-wave schedule, then fixed chunks around the
+                // default chunk length
                 const int z0 = default_zchunk(s->P.nx, s->P.ny, s->P.nz, t[0], t[1], s->num_sms);
-                int zs[3] = {z0, std::max(4, z0 / 2), std::min(s->P.nz, 2 * z0)};
-                for (int zi = 0; zi < 3 && status == LBMAN_OK; ++zi) {
-                    if (zi > 0 && (zs[zi] == z0 || (zi == 2 && zs[2] == zs[1]))) continue;
+                int zs[6] = {0, -2, -3, z0, std::max(4, z0 / 2), std::min(s->P.nz, 2 * z0)};
+                for (int zi = 0; zi < 6 && status == LBMAN_OK; ++zi) {
+                    if (zi > 3 && (zs[zi] == z0 || (zi == 5 && zs[5] == zs[4]))) continue;
                     cur = {k, t[0], t[1], zs[zi], 0, 0.0};
                     if (lbman_set_shape(s, &cur) != LBMAN_OK) continue;
                     if ((status = one_step(s, false)) != LBMAN_OK) break;

@@ -43,8 +43,11 @@ __global__ void __launch_bounds__(TL::NT, (Stage<TL, R>::MINB)) ens_qforce_kerne
     for (int w = blockIdx.x; w < nwork; w += gridDim.x) {
         const EnsQWork it = work[w];
         const EnsBox& B = boxes[it.box];
-        qf_march<TL, R, UPWIND>(B.P, B.zc, (const R*)B.q[par], (const R*)B.u[0], reinterpret_cast<R*>(smem_raw),
-                                StoreQForce<R>{(R*)B.q[1 - par], (R*)B.F, B.P.V}, it.bx, it.by, it.bz);
+        const int z0 = it.bz * B.zc;
+        if (z0 < B.P.nz)
+            qf_march<TL, R, UPWIND>(B.P, it.bx * TL::TCX, it.by * TL::TCY, z0, min(z0 + B.zc, B.P.nz),
+                                    (const R*)B.q[par], (const R*)B.u[0], reinterpret_cast<R*>(smem_raw),
+                                    StoreQForce<R>{(R*)B.q[1 - par], (R*)B.F, B.P.V});
         __syncthreads();  // the staging rings are reused by the next item
     }
 }
@@ -57,11 +60,13 @@ __global__ void __launch_bounds__(TL::NT) ens_fused_kernel(const EnsBox* __restr
     for (int w = blockIdx.x; w < nwork; w += gridDim.x) {
         const EnsQWork it = work[w];
         const EnsBox& B = boxes[it.box];
-        qf_march<TL, R, UPWIND>(B.P, B.zc, (const R*)B.q[par], (const R*)B.u[par], reinterpret_cast<R*>(smem_raw),
-                                CollideCell<R, S, DEV>{B.P, phys_ref<R>(B.P), first, (R*)B.q[1 - par],
-                                                       (R*)B.u[1 - par], (const S*)B.f[par], (S*)B.f[1 - par],
-                                                       (R*)B.rho, nullptr, write_rho_all},
-                                it.bx, it.by, it.bz);
+        const int z0 = it.bz * B.zc;
+        if (z0 < B.P.nz)
+            qf_march<TL, R, UPWIND>(B.P, it.bx * TL::TCX, it.by * TL::TCY, z0, min(z0 + B.zc, B.P.nz),
+                                    (const R*)B.q[par], (const R*)B.u[par], reinterpret_cast<R*>(smem_raw),
+                                    CollideCell<R, S, DEV>{B.P, phys_ref<R>(B.P), first, (R*)B.q[1 - par],
+                                                           (R*)B.u[1 - par], (const S*)B.f[par],
+                                                           (S*)B.f[1 - par], (R*)B.rho, nullptr, write_rho_all});
         __syncthreads();
     }
 }

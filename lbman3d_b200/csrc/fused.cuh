@@ -63,10 +63,9 @@ __global__ void __launch_bounds__(TL::NT) fused_kernel(const __grid_constant__ S
                                                        R* __restrict__ rho_buf, R* __restrict__ Fout,
                                                        int write_rho_all) {
     extern __shared__ __align__(16) unsigned char smem_raw[];
-    qf_march<TL, R, UPWIND>(
+    qf_run<TL, R, UPWIND>(
         P, zc_len, qin, uin, reinterpret_cast<R*>(smem_raw),
-        CollideCell<R, S, DEV>{P, phys_ref<R>(P), first, qout, uout, fin, fout, rho_buf, Fout, write_rho_all},
-        blockIdx.x, blockIdx.y, blockIdx.z);
+        CollideCell<R, S, DEV>{P, phys_ref<R>(P), first, qout, uout, fin, fout, rho_buf, Fout, write_rho_all});
 }
 
 }  // namespace lbman

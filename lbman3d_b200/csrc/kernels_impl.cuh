@@ -8,6 +8,8 @@
 #include "reduce.cuh"
 #include "tiles.h"
 
+#include <algorithm>
+#include <atomic>
 #include <utility>
 
 namespace lbman {
@@ -59,19 +61,49 @@ int qforce_threads(const QTile& T) {
     return n;
 }
 
+// Resident blocks per SM of one kernel instantiation at its launch shape
+// (queried once; the dynamic shared-memory limit is raised by prepare()).
+template <auto Kern>
+int resident_blocks(int threads, size_t smem) {
+    static std::atomic<int> cached{0};
+    int n = cached.load(std::memory_order_relaxed);
+    if (n == 0) {
+        if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, Kern, threads, smem) != cudaSuccess || n < 1) {
+            cudaGetLastError();
+            n = 1;
+        }
+        cached.store(n, std::memory_order_relaxed);
+    }
+    return n;
+}
+
+// Grid of a z-marching launch: fixed z chunks (zc > 0), or for the balanced
+// schedule (zc <= 0) max(1, -zc) waves of resident blocks sharing the
+// (column, plane) units equally.
+template <class TL, auto Kern>
+dim3 march_grid(const SimParams& P, const LaunchShape& S, size_t smem) {
+    if (S.tile.zc > 0) return qgrid(P, TL::TCX, TL::TCY, S.tile.zc);
+    const int64_t units = (int64_t)((P.nx + TL::TCX - 1) / TL::TCX) * ((P.ny + TL::TCY - 1) / TL::TCY) * P.nz;
+    const int64_t waves = std::max(1, -S.tile.zc);
+    const int64_t grid = waves * resident_blocks<Kern>(TL::NT, smem) * S.num_sms;
+    return dim3((unsigned)std::max<int64_t>(1, std::min(units, grid)));
+}
+
 template <class R>
 cudaError_t qforce(const SimParams& P, const LaunchShape& S, const void* qin, const void* uin, void* qout,
                    void* Fout, cudaStream_t st) {
     return with_tile<R>(S.tile.tcx, S.tile.tcy, [&](auto tl) {
         using TL = decltype(tl);
-        const dim3 g = qgrid(P, TL::TCX, TL::TCY, S.tile.zc);
         const size_t smem = TL::template smem_bytes<R>();
-        if (P.upwind)
-            qforce_kernel<TL, R, true><<<g, TL::NT, smem, st>>>(P, S.tile.zc, (const R*)qin, (const R*)uin,
-                                                               (R*)qout, (R*)Fout);
-        else
-            qforce_kernel<TL, R, false><<<g, TL::NT, smem, st>>>(P, S.tile.zc, (const R*)qin, (const R*)uin,
-                                                                (R*)qout, (R*)Fout);
+        if (P.upwind) {
+            constexpr auto K = qforce_kernel<TL, R, true>;
+            K<<<march_grid<TL, K>(P, S, smem), TL::NT, smem, st>>>(P, S.tile.zc, (const R*)qin, (const R*)uin,
+                                                                   (R*)qout, (R*)Fout);
+        } else {
+            constexpr auto K = qforce_kernel<TL, R, false>;
+            K<<<march_grid<TL, K>(P, S, smem), TL::NT, smem, st>>>(P, S.tile.zc, (const R*)qin, (const R*)uin,
+                                                                   (R*)qout, (R*)Fout);
+        }
         return cudaGetLastError();
     });
 }
@@ -82,18 +114,40 @@ cudaError_t fused(const SimParams& P, const LaunchShape& L, bool first, const vo
                   cudaStream_t st) {
     return with_tile<R>(L.tile.tcx, L.tile.tcy, [&](auto tl) {
         using TL = decltype(tl);
-        const dim3 g = qgrid(P, TL::TCX, TL::TCY, L.tile.zc);
         const size_t smem = TL::template smem_bytes<R>();
-        auto launch = [&](auto kern) {
+        auto launch = [&](auto kern, dim3 g) {
             kern<<<g, TL::NT, smem, st>>>(P, L.tile.zc, first ? 1 : 0, (const R*)qin, (const R*)uin, (R*)qout,
                                           (R*)uout, (const S*)fin, (S*)fout, (R*)rho, (R*)Fout, wr ? 1 : 0);
         };
-        if (P.upwind)
-            launch(fused_kernel<TL, R, S, DEV, true>);
-        else
-            launch(fused_kernel<TL, R, S, DEV, false>);
+        if (P.upwind) {
+            constexpr auto K = fused_kernel<TL, R, S, DEV, true>;
+            launch(K, march_grid<TL, K>(P, L, smem));
+        } else {
+            constexpr auto K = fused_kernel<TL, R, S, DEV, false>;
+            launch(K, march_grid<TL, K>(P, L, smem));
+        }
         return cudaGetLastError();
     });
+}
+
+// Blocks of the Q+force (or fused) launch for this shape.
+template <class R, class S, bool DEV>
+int march_blocks(const SimParams& P, const LaunchShape& L, bool fused_org) {
+    int n = 0;
+    with_tile<R>(L.tile.tcx, L.tile.tcy, [&](auto tl) {
+        using TL = decltype(tl);
+        const size_t smem = TL::template smem_bytes<R>();
+        dim3 g;
+        if (fused_org)
+            g = P.upwind ? march_grid<TL, fused_kernel<TL, R, S, DEV, true>>(P, L, smem)
+                         : march_grid<TL, fused_kernel<TL, R, S, DEV, false>>(P, L, smem);
+        else
+            g = P.upwind ? march_grid<TL, qforce_kernel<TL, R, true>>(P, L, smem)
+                         : march_grid<TL, qforce_kernel<TL, R, false>>(P, L, smem);
+        n = (int)(g.x * g.y * g.z);
+        return cudaSuccess;
+    });
+    return n;
 }
 
 template <class R, class S, bool DEV>
@@ -279,5 +333,8 @@ cudaError_t prepare(size_t max_smem) {
     }                                                                                                   \
     size_t qforce_smem_##SUF(const QTile& T) { return impl::qforce_smem<R>(T); }                       \
     int qforce_threads_##SUF(const QTile& T) { return impl::qforce_threads<R>(T); }                    \
+    int march_blocks_##SUF(const SimParams& P, const LaunchShape& shape, bool fused_org) {             \
+        return impl::march_blocks<R, S, DEV>(P, shape, fused_org);                                      \
+    }                                                                                                   \
     cudaError_t prepare_##SUF(size_t max_smem) { return impl::prepare<R, S, DEV>(max_smem); }           \
     }

@@ -14,8 +14,9 @@ namespace lbman {
 // Work shape of one step; filled by the host layer from the grid size and the
 // autotuner.
 struct LaunchShape {
-    QTile tile;
+    QTile tile;        // tile.zc == 0: balanced one-wave schedule
     int qthreads;
+    int num_sms = 148;  // multiprocessors of the device (sizes the balanced grid)
 };
 
 #define LBMAN_DECLARE_LAUNCHERS(SUF)                                                                   \
@@ -49,6 +50,7 @@ struct LaunchShape {
                                          void* rho, void* u, void* q, void* F, cudaStream_t st);       \
     size_t qforce_smem_##SUF(const QTile& T);                                                          \
     int qforce_threads_##SUF(const QTile& T);                                                          \
+    int march_blocks_##SUF(const SimParams& P, const LaunchShape& shape, bool fused_org);              \
     cudaError_t prepare_##SUF(size_t max_smem);
 
 LBMAN_DECLARE_LAUNCHERS(f64)

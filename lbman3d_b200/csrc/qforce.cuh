@@ -359,19 +359,16 @@ __device__ __forceinline__ void qf_force_cell(const SimParams& P, const Phys<R>&
     }
 }
 
-// Marches a block through its z chunk.  The copy of plane zc+3 is in flight
-// while planes zc+1 (results) and zc (force, consumer) are computed.
+// Marches a block through planes [z0, z1) of the column at (x0, y0).  The
+// copy of plane zc+3 is in flight while planes zc+1 (results) and zc (force,
+// consumer) are computed.
 template <class TL, class R, bool UPWIND, class OutFn>
-__device__ __forceinline__ void qf_march(const SimParams& P, int zc_len, const R* __restrict__ qin,
-                                         const R* __restrict__ uin, R* smem, OutFn&& out, int bx, int by,
-                                         int bz) {
+__device__ __forceinline__ void qf_march(const SimParams& P, int x0, int y0, int z0, int z1,
+                                         const R* __restrict__ qin, const R* __restrict__ uin, R* smem,
+                                         OutFn&& out) {
     using ST = Stage<TL, R>;
     R* QU = smem;
     R* Bs = smem + 4 * 8 * ST::NQU;
-    const int x0 = bx * TL::TCX, y0 = by * TL::TCY;
-    const int z0 = bz * zc_len;
-    if (z0 >= P.nz) return;
-    const int z1 = min(z0 + zc_len, P.nz);
     const Phys<R>& K = phys_ref<R>(P);
     const PointGeo G = point_geo<TL>(P, x0, y0, z0, z1);
     const AxisRule qx = q_rule(P, 0, G.ax, P.nx), qy = q_rule(P, 1, G.ay, P.ny);
@@ -404,6 +401,37 @@ __device__ __forceinline__ void qf_march(const SimParams& P, int zc_len, const R
     }
 }
 
+// Work of one block of a single-box launch.  zc_len > 0: block (bx, by, bz)
+// marches z chunk bz of column (bx, by).  zc_len <= 0 (balanced): the grid is
+// a whole number of waves of resident blocks, and block b takes the b-th
+// equal share of the column-major sequence of (column, plane) units -- one
+// or two partial columns -- so blocks finish within a plane of each other
+// and no partial last wave idles the SMs.
+template <class TL, class R, bool UPWIND, class OutFn>
+__device__ __forceinline__ void qf_run(const SimParams& P, int zc_len, const R* __restrict__ qin,
+                                       const R* __restrict__ uin, R* smem, OutFn&& out) {
+    if (zc_len > 0) {
+        const int z0 = blockIdx.z * zc_len;
+        if (z0 >= P.nz) return;
+        qf_march<TL, R, UPWIND>(P, blockIdx.x * TL::TCX, blockIdx.y * TL::TCY, z0, min(z0 + zc_len, P.nz), qin,
+                                uin, smem, out);
+        return;
+    }
+    const int cx = (P.nx + TL::TCX - 1) / TL::TCX, cy = (P.ny + TL::TCY - 1) / TL::TCY;
+    const int64_t W = (int64_t)cx * cy * P.nz;
+    int64_t w = W * blockIdx.x / gridDim.x;
+    const int64_t w1 = W * (blockIdx.x + 1) / gridDim.x;
+    while (w < w1) {
+        const int64_t col = w / P.nz;
+        const int z0 = (int)(w - col * P.nz);
+        const int z1 = (int)min((int64_t)P.nz, z0 + (w1 - w));
+        const int by = (int)(col / cx), bx = (int)(col - (int64_t)by * cx);
+        qf_march<TL, R, UPWIND>(P, bx * TL::TCX, by * TL::TCY, z0, z1, qin, uin, smem, out);
+        __syncthreads();  // the staging rings are reused by the next segment
+        w += z1 - z0;
+    }
+}
+
 // Consumer of the split organisation: store Q_new and the body force.
 template <class R>
 struct StoreQForce {
@@ -424,8 +452,7 @@ __global__ void __launch_bounds__(TL::NT, (Stage<TL, R>::MINB)) qforce_kernel(co
                                                         const R* __restrict__ qin, const R* __restrict__ uin,
                                                         R* __restrict__ qout, R* __restrict__ Fout) {
     extern __shared__ __align__(16) unsigned char smem_raw[];
-    qf_march<TL, R, UPWIND>(P, zc_len, qin, uin, reinterpret_cast<R*>(smem_raw), StoreQForce<R>{qout, Fout, P.V},
-                            blockIdx.x, blockIdx.y, blockIdx.z);
+    qf_run<TL, R, UPWIND>(P, zc_len, qin, uin, reinterpret_cast<R*>(smem_raw), StoreQForce<R>{qout, Fout, P.V});
 }
 
 }  // namespace lbman

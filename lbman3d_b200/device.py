@@ -130,6 +130,31 @@ class Simulation:
             N.check(st)
         return {k: getattr(d, k) for k, _ in N.lbman_diag._fields_}
 
+    def default_bins(self) -> int:
+        """Shell count that covers every wavevector / separation of the box."""
+        return int(max(self.params.nx, self.params.ny, self.params.nz) * 3 ** 0.5 / 2) + 2
+
+    def velocity_spectrum(self, nbins: int = None):
+        """Shell-averaged kinetic-energy spectrum E[b] and wavevectors per shell."""
+        nb = int(nbins or self.default_bins())
+        E, n = np.zeros(nb), np.zeros(nb)
+        N.check(N.lib().lbman_velocity_spectrum(self._h, nb, N.dptr(E), N.dptr(n)))
+        return E, n
+
+    def q_correlation(self, nbins: int = None):
+        """Radially averaged Q autocorrelation C[b], separations per shell and
+        the 1/e correlation length (-1 if not reached)."""
+        nb = int(nbins or self.default_bins())
+        Cb, n, xi = np.zeros(nb), np.zeros(nb), C.c_double()
+        N.check(N.lib().lbman_q_correlation(self._h, nb, N.dptr(Cb), N.dptr(n), C.byref(xi)))
+        return Cb, n, xi.value
+
+    def statistics(self) -> dict:
+        """Mean and rms speed, defect plaquettes and their density per cell."""
+        st = N.lbman_stats()
+        N.check(N.lib().lbman_statistics(self._h, C.byref(st)))
+        return {k: getattr(st, k) for k, _ in N.lbman_stats._fields_}
+
     def shape(self) -> dict:
         s = N.lbman_shape()
         N.check(N.lib().lbman_get_shape(self._h, C.byref(s)))
