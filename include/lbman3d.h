@@ -269,6 +269,62 @@ typedef struct lbman_stats {
 } lbman_stats;
 int lbman_statistics(lbman_solver* s, lbman_stats* out);
 
+/* Learned closure (no counterpart in the reference).
+ *
+ * Tensor-core self-test: one 128x32x64 BF16 GEMM with FP32 accumulation
+ * through tcgen05 for each of the four operand-major combinations (A, B each
+ * K- or MN-major), compared with an FP64 host product of the same BF16
+ * inputs.  max_rel_err[4] (may be NULL) receives max |D - D_ref| / sum |a b|
+ * per combination (-1 if the device wait timed out).                       */
+int lbman_closure_selftest(int device, double* max_rel_err);
+
+/* The closure network: 4 periodic 3x3x3 convolutions, 9 -> 32 -> 32 -> 32 -> 8
+ * channels, GELU after the first three; BF16 weights and activations, FP32
+ * accumulation, forward and backward on tcgen05 tensor cores.  Inputs are
+ * the coarse rho, u (3) and Q (5), normalised per channel by (x - shift) /
+ * scale; outputs are corrections to Q (5) and u (3) in units of out_scale.
+ * The handle owns the network for one coarse grid size, Adam state and a
+ * device-resident training set of box-filtered fine snapshots.             */
+typedef struct lbman_closure lbman_closure;
+int lbman_closure_create(int device, int nx, int ny, int nz, uint64_t seed, lbman_closure** out);
+int lbman_closure_destroy(lbman_closure* c);
+/* Parameters as one FP32 vector: per layer W[27][cin][cout] (cin 16, 32,
+ * 32, 32; cout 32, 32, 32, 16; tap = (dz+1)*9 + (dy+1)*3 + (dx+1)) then
+ * b[cout]; padding entries (layer-0 inputs 9..15, layer-3 outputs 8..15)
+ * are held at zero.                                                       */
+int lbman_closure_param_count(void);
+int lbman_closure_get_params(lbman_closure* c, float* params);
+int lbman_closure_set_params(lbman_closure* c, const float* params);
+int lbman_closure_get_scales(lbman_closure* c, float* shift9, float* scale9, float* out_scale8);
+int lbman_closure_set_scales(lbman_closure* c, const float* shift9, const float* scale9, const float* out_scale8);
+/* Network on host fields feat9 [9][V] (rho, u, Q); out8 [8][V] receives the
+ * normalised outputs.                                                       */
+int lbman_closure_forward(lbman_closure* c, const float* feat9, float* out8);
+/* Loss (1/8V) sum_c sum_j (out_j - target_j / out_scale_j)^2 for raw targets
+ * target8 [8][V], and its gradient with respect to every parameter
+ * (grad may be NULL), without updating anything.                          */
+int lbman_closure_gradient(lbman_closure* c, const float* feat9, const float* target8, double* loss, float* grad);
+/* Appends the box-filtered state of an FP32/FP16 fine solver whose grid is
+ * f times the closure grid on every axis; new_trajectory starts a new
+ * sequence (pairs never span two sequences).                              */
+int lbman_closure_record(lbman_closure* c, lbman_solver* fine, int new_trajectory);
+int lbman_closure_dataset(lbman_closure* c, int* snapshots, int* pairs);
+/* For each consecutive snapshot pair (k, k+1) of a sequence, the target
+ * snapshot(k+1) - coarse_step(snapshot k), where coarse_step rebuilds the
+ * populations as f_eq and takes one step of the coarse solver (FP32/FP16 on
+ * the closure grid, with the coarse-grid parameters).  fit_scales sets the
+ * input shift/scale to the per-channel mean/std of the snapshots and the
+ * output scales to the rms target of Q and of u.                          */
+int lbman_closure_build_targets(lbman_closure* c, lbman_solver* coarse, int fit_scales);
+/* Adam (beta 0.9 / 0.999) on random training pairs; loss_first/last receive
+ * the mean loss of the first and last tenth of the iterations.            */
+int lbman_closure_train(lbman_closure* c, int iters, float lr, uint64_t seed, double* loss_first, double* loss_last);
+/* Coarse solver state := snapshot k.                                        */
+int lbman_closure_load_snapshot(lbman_closure* c, int k, lbman_solver* coarse);
+/* nsteps corrected coarse steps: network on the current state, populations
+ * rebuilt as f_eq, one solver step, then Q and u corrected.               */
+int lbman_closure_step(lbman_closure* c, lbman_solver* coarse, int nsteps);
+
 /* Steps completed since the last upload. */
 int lbman_steps_done(lbman_solver* s, int64_t* steps);
 /* Kernel launches issued by this solver since creation (instrumentation).  */

@@ -71,6 +71,7 @@ _lib = None
 
 # (name, restype, argtypes) for every entry point declared in include/lbman3d.h
 _DP = C.POINTER(C.c_double)
+_FP = C.POINTER(C.c_float)
 PROTOTYPES = [
     ("lbman_config_init", C.c_int, [C.POINTER(lbman_config)]),
     ("lbman_status_string", C.c_char_p, [C.c_int]),
@@ -109,6 +110,22 @@ PROTOTYPES = [
     ("lbman_velocity_spectrum", C.c_int, [C.c_void_p, C.c_int, _DP, _DP]),
     ("lbman_q_correlation", C.c_int, [C.c_void_p, C.c_int, _DP, _DP, _DP]),
     ("lbman_statistics", C.c_int, [C.c_void_p, C.POINTER(lbman_stats)]),
+    ("lbman_closure_selftest", C.c_int, [C.c_int, _DP]),
+    ("lbman_closure_create", C.c_int, [C.c_int, C.c_int, C.c_int, C.c_int, C.c_uint64, C.POINTER(C.c_void_p)]),
+    ("lbman_closure_destroy", C.c_int, [C.c_void_p]),
+    ("lbman_closure_param_count", C.c_int, []),
+    ("lbman_closure_get_params", C.c_int, [C.c_void_p, _FP]),
+    ("lbman_closure_set_params", C.c_int, [C.c_void_p, _FP]),
+    ("lbman_closure_get_scales", C.c_int, [C.c_void_p, _FP, _FP, _FP]),
+    ("lbman_closure_set_scales", C.c_int, [C.c_void_p, _FP, _FP, _FP]),
+    ("lbman_closure_forward", C.c_int, [C.c_void_p, _FP, _FP]),
+    ("lbman_closure_gradient", C.c_int, [C.c_void_p, _FP, _FP, _DP, _FP]),
+    ("lbman_closure_record", C.c_int, [C.c_void_p, C.c_void_p, C.c_int]),
+    ("lbman_closure_dataset", C.c_int, [C.c_void_p, C.POINTER(C.c_int), C.POINTER(C.c_int)]),
+    ("lbman_closure_build_targets", C.c_int, [C.c_void_p, C.c_void_p, C.c_int]),
+    ("lbman_closure_train", C.c_int, [C.c_void_p, C.c_int, C.c_float, C.c_uint64, _DP, _DP]),
+    ("lbman_closure_load_snapshot", C.c_int, [C.c_void_p, C.c_int, C.c_void_p]),
+    ("lbman_closure_step", C.c_int, [C.c_void_p, C.c_void_p, C.c_int]),
     ("lbman_flow_reduce_noalloc", C.c_int,
      [C.c_int64, C.c_int, C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p, C.POINTER(lbman_diag)]),
 ]
@@ -137,6 +154,15 @@ def check(status: int):
             raise DivergedError(status, msg)
         raise LbmanError(status, msg)
     return status
+
+
+def fptr(a):
+    """float32 C-contiguous numpy array -> float*, None -> NULL."""
+    if a is None:
+        return None
+    if a.dtype.name != "float32" or not a.flags.c_contiguous:
+        raise TypeError("buffers must be C-contiguous float32 arrays")
+    return a.ctypes.data_as(_FP)
 
 
 def dptr(a):

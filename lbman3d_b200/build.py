@@ -42,6 +42,7 @@ UNITS = {
     "ens_api.cu": [],
     "noalloc.cu": [],
     "stats.cu": [],
+    "closure_api.cu": [],
 }
 
 

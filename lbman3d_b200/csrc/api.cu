@@ -11,6 +11,7 @@
 
 #include "../../include/lbman3d.h"
 #include "launch.h"
+#include "solver_view.h"
 #include "stats.h"
 #include "tiles.h"
 
@@ -454,6 +455,51 @@ int lbman_upload(lbman_solver* s, const double* rho, const double* u3, const dou
     s->steps = 0;
     return LBMAN_OK;
 }
+
+}  // extern "C"
+
+namespace lbman {
+
+int solver_view(lbman_solver* s, SolverView* v) {
+    if (!s || !v) return fail(LBMAN_ERR_ARG, "null argument");
+    v->prec = s->prec;
+    v->nx = s->P.nx;
+    v->ny = s->P.ny;
+    v->nz = s->P.nz;
+    v->V = s->P.V;
+    v->rho = s->rho;
+    v->u = s->u[s->ucur];
+    v->q = s->q[s->qcur];
+    v->stream = s->stream;
+    v->uploaded = s->uploaded;
+    return LBMAN_OK;
+}
+
+int solver_reset_populations(lbman_solver* s) {
+    if (!s) return fail(LBMAN_ERR_ARG, "null solver");
+    if (!s->uploaded) return fail(LBMAN_ERR_STATE, "no state to rebuild populations from");
+    LB_TRY(set_device(s));
+    LB_TRY(check_launch(s, s->ops().feq_init(s->P, s->rho, s->u[s->ucur], s->f[s->fcur], s->stream), "feq_init"));
+    s->f_post = false;
+    return LBMAN_OK;
+}
+
+int solver_set_state(lbman_solver* s, const void* rho, const void* u3, const void* q5) {
+    if (!s || !rho || !u3 || !q5) return fail(LBMAN_ERR_ARG, "null argument");
+    LB_TRY(set_device(s));
+    const int64_t V = s->P.V;
+    LB_CUDA(cudaMemcpyAsync(s->rho, rho, V * s->rbytes, cudaMemcpyDeviceToDevice, s->stream));
+    LB_CUDA(cudaMemcpyAsync(s->u[s->ucur], u3, 3 * V * s->rbytes, cudaMemcpyDeviceToDevice, s->stream));
+    LB_CUDA(cudaMemcpyAsync(s->q[s->qcur], q5, 5 * V * s->rbytes, cudaMemcpyDeviceToDevice, s->stream));
+    LB_CUDA(cudaMemsetAsync(s->F, 0, 3 * V * s->rbytes, s->stream));
+    s->uploaded = true;
+    s->steps = 0;
+    return solver_reset_populations(s);
+}
+
+}  // namespace lbman
+
+extern "C" {
 
 int lbman_init_seeded(lbman_solver* s, uint64_t seed, double S0, double sigma) {
     if (!s) return fail(LBMAN_ERR_ARG, "null solver");

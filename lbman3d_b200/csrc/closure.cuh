@@ -1,0 +1,542 @@
+// closure.cuh -- kernels of the learned closure: a 4-layer 3x3x3 periodic
+// convolutional network (9 -> 32 -> 32 -> 32 -> 8 channels, GELU after the
+// first three layers) on a coarse grid, with BF16 operands on the tcgen05
+// tensor cores and FP32 accumulation in TMEM.  No counterpart in the
+// reference.
+//
+// Activations are channel-last BF16, act[cell][C] with C = 16 (the 9 input
+// features, zero padded) or 32; the last layer's 8 outputs are padded to 16.
+// A convolution is an implicit GEMM: for a tile of 128 cells (M) and each of
+// the 27 taps, the 128 x CIN neighbour rows are gathered into shared memory
+// (K-major) and multiplied by that tap's CIN x COUT weights (N = COUT), all
+// 27 taps accumulating into one TMEM accumulator.  Two A stages let the
+// gather of tap t+1 overlap the MMAs of tap t.  The backward data pass is
+// the same kernel run with the transposed, tap-reversed weight image; the
+// weight gradient is a GEMM over cells (K) with M = (tap, ci) rows and
+// MN-major operands taken straight from the channel-last activations.
+//
+// Tap index: tap = (dz+1)*9 + (dy+1)*3 + (dx+1); output cell c reads input
+// cell c + (dx, dy, dz) with periodic wrap on every axis.
+#pragma once
+
+#include <cuda_bf16.h>
+#include <stdint.h>
+
+#include "tc.cuh"
+
+namespace lbman {
+namespace cl {
+
+constexpr int kTileM = 128;
+constexpr int kThreads = 128;
+
+struct Grid3 {
+    int nx, ny, nz;
+    int64_t V;
+};
+
+__device__ __forceinline__ int wrapi(int a, int n) { return a < 0 ? a + n : (a >= n ? a - n : a); }
+
+__device__ __forceinline__ int64_t neighbour(const Grid3& g, int x, int y, int z, int tap) {
+    const int dx = tap % 3 - 1, dy = (tap / 3) % 3 - 1, dz = tap / 9 - 1;
+    return ((int64_t)wrapi(z + dz, g.nz) * g.ny + wrapi(y + dy, g.ny)) * g.nx + wrapi(x + dx, g.nx);
+}
+
+__device__ __forceinline__ float gelu(float x) { return 0.5f * x * (1.0f + erff(x * 0.70710678118654752f)); }
+__device__ __forceinline__ float gelu_grad(float x) {
+    const float cdf = 0.5f * (1.0f + erff(x * 0.70710678118654752f));
+    const float pdf = 0.39894228040143268f * expf(-0.5f * x * x);
+    return cdf + x * pdf;
+}
+
+// Byte size of the B image of one convolution: 27 taps x CIN/16 k-steps of
+// COUT x 16 K-major BF16 (core matrices: n-group stride 256, k-group 128).
+__host__ __device__ constexpr int bimg_bytes(int cin, int cout) { return 27 * (cin / 16) * cout * 32; }
+
+enum ConvMode : int {
+    kFwdHidden = 0,  // + bias, store pre (BF16) and GELU(pre) (BF16)
+    kFwdLast = 1,    // + bias, store FP32
+    kBwdData = 2     // times GELU'(pre of the layer below), store BF16
+};
+
+// One persistent CTA walks 128-cell tiles.  Smem: B image, then 2 A stages
+// of CIN/16 x 4 KB.
+template <int CIN, int COUT, int MODE>
+__global__ void __launch_bounds__(kThreads) conv_kernel(Grid3 g, const __nv_bfloat16* __restrict__ in,
+                                                        const uint4* __restrict__ bimg, const float* __restrict__ bias,
+                                                        const __nv_bfloat16* __restrict__ pre_below,
+                                                        __nv_bfloat16* __restrict__ out_pre,
+                                                        __nv_bfloat16* __restrict__ out_bf, float* __restrict__ out_f,
+                                                        int* __restrict__ err) {
+    constexpr int KS = CIN / 16;                 // k-steps per tap
+    constexpr int BBYTES = bimg_bytes(CIN, COUT);
+    constexpr int ABYTES = KS * 4096;            // one A stage
+    extern __shared__ __align__(1024) unsigned char sm[];
+    __shared__ uint64_t bar[2];
+    __shared__ uint32_t tslot;
+    unsigned char* Bs = sm;
+    unsigned char* As = sm + BBYTES;
+    const int t = threadIdx.x;
+
+    for (int i = t; i < BBYTES / 16; i += kThreads) reinterpret_cast<uint4*>(Bs)[i] = bimg[i];
+    if (t == 0) {
+        tc::mbar_init(&bar[0], 1);
+        tc::mbar_init(&bar[1], 1);
+        tc::mbar_fence_init();
+    }
+    if (t < 32) tc::tmem_alloc(&tslot, 32);
+    tc::fence_smem_async();
+    tc::fence_before_sync();
+    __syncthreads();
+    tc::fence_after_sync();
+    const uint32_t tmem = tslot;
+    const uint32_t idesc = tc::idesc_bf16(kTileM, COUT, 0, 0);
+    const uint32_t a0 = tc::smem_addr(As), b0 = tc::smem_addr(Bs);
+    uint32_t uses[2] = {0, 0};  // commits issued per A stage (same in every thread)
+    bool ok = true;
+
+    const int64_t ntiles = (g.V + kTileM - 1) / kTileM;
+    for (int64_t tile = blockIdx.x; tile < ntiles && ok; tile += gridDim.x) {
+        const int64_t c = tile * kTileM + t;
+        const bool live = c < g.V;
+        const int64_t cc = live ? c : 0;
+        const int x = (int)(cc % g.nx), y = (int)((cc / g.nx) % g.ny), z = (int)(cc / ((int64_t)g.nx * g.ny));
+        for (int tap = 0; tap < 27; ++tap) {
+            const int s = tap & 1;
+            // stage s is free once the MMAs that read it last have completed
+            bool lost = uses[s] > 0 && !tc::mbar_wait(&bar[s], (uses[s] - 1) & 1, err);
+            if (__syncthreads_or(lost)) {
+                ok = false;
+                break;
+            }
+            // gather this row's CIN channels of the neighbour into stage s
+            const uint4* src = reinterpret_cast<const uint4*>(in + neighbour(g, x, y, z, tap) * CIN);
+            unsigned char* dst = As + s * ABYTES + (t / 8) * 256 + (t % 8) * 16;
+#pragma unroll
+            for (int q = 0; q < CIN / 8; ++q)
+                *reinterpret_cast<uint4*>(dst + (q / 2) * 4096 + (q % 2) * 128) = src[q];
+            tc::fence_smem_async();
+            tc::fence_before_sync();
+            __syncthreads();
+            tc::fence_after_sync();
+            if (t == 0) {
+#pragma unroll
+                for (int kb = 0; kb < KS; ++kb) {
+                    const uint64_t da = tc::smem_desc(a0 + s * ABYTES + kb * 4096, 128, 256);
+                    const uint64_t db = tc::smem_desc(b0 + (tap * KS + kb) * COUT * 32, 128, 256);
+                    tc::mma_bf16(tmem, da, db, idesc, (tap > 0 || kb > 0) ? 1u : 0u);
+                }
+                tc::mma_commit(&bar[s]);
+            }
+            ++uses[s];
+        }
+        if (!ok) break;
+        // the last commit (tap 26, stage 0) covers every MMA of the tile
+        const bool lost = !tc::mbar_wait(&bar[0], (uses[0] - 1) & 1, err);
+        if (__syncthreads_or(lost)) {
+            ok = false;
+            break;
+        }
+        tc::fence_after_sync();
+        const int w = t >> 5;
+        float acc[COUT];
+#pragma unroll
+        for (int c0 = 0; c0 < COUT; c0 += 16) tc::tmem_ld16(tmem + ((uint32_t)(32 * w) << 16) + (uint32_t)c0, acc + c0);
+        if (live) {
+            if constexpr (MODE == kFwdHidden) {
+                __align__(16) __nv_bfloat16 pb[COUT], ab[COUT];
+#pragma unroll
+                for (int j = 0; j < COUT; ++j) {
+                    const float p = acc[j] + bias[j];
+                    pb[j] = __float2bfloat16(p);
+                    ab[j] = __float2bfloat16(gelu(p));
+                }
+#pragma unroll
+                for (int q = 0; q < COUT / 8; ++q) {
+                    reinterpret_cast<uint4*>(out_pre + c * COUT)[q] = reinterpret_cast<const uint4*>(pb)[q];
+                    reinterpret_cast<uint4*>(out_bf + c * COUT)[q] = reinterpret_cast<const uint4*>(ab)[q];
+                }
+            } else if constexpr (MODE == kFwdLast) {
+#pragma unroll
+                for (int j = 0; j < COUT; j += 4)
+                    reinterpret_cast<float4*>(out_f + c * COUT)[j / 4] =
+                        make_float4(acc[j] + bias[j], acc[j + 1] + bias[j + 1], acc[j + 2] + bias[j + 2],
+                                    acc[j + 3] + bias[j + 3]);
+            } else {
+                __align__(16) __nv_bfloat16 pre[COUT], gb[COUT];
+#pragma unroll
+                for (int q = 0; q < COUT / 8; ++q)
+                    reinterpret_cast<uint4*>(pre)[q] = reinterpret_cast<const uint4*>(pre_below + c * COUT)[q];
+#pragma unroll
+                for (int j = 0; j < COUT; ++j) gb[j] = __float2bfloat16(acc[j] * gelu_grad(__bfloat162float(pre[j])));
+#pragma unroll
+                for (int q = 0; q < COUT / 8; ++q)
+                    reinterpret_cast<uint4*>(out_bf + c * COUT)[q] = reinterpret_cast<const uint4*>(gb)[q];
+            }
+        }
+        tc::fence_before_sync();
+        __syncthreads();  // TMEM reads done before the next tile's first MMA
+        tc::fence_after_sync();
+    }
+    // drain: never leave with MMAs in flight on our TMEM
+    if (t == 0) {
+        for (int s = 0; s < 2; ++s)
+            if (uses[s] > 0) tc::mbar_wait(&bar[s], (uses[s] - 1) & 1, err);
+    }
+    tc::fence_before_sync();
+    __syncthreads();
+    if (t < 32) tc::tmem_dealloc(tmem, 32);
+}
+
+// Weight gradient dW[tap][ci][co] = sum_c act[c + off(tap)][ci] * grad[c][co]
+// over this CTA's cell range, as partials[cta][tap][ci][co] (FP32).
+// M rows = (tap-in-group j, ci), TPG = 128/CIN taps per group, G groups;
+// K = cells, 32 per stage (2 k-steps); operands MN-major.
+template <int CIN, int COUT>
+struct WGradShape {
+    static constexpr int TPG = kTileM / CIN;
+    static constexpr int G = (27 + TPG - 1) / TPG;
+    static constexpr int COLS = G * COUT;
+    static constexpr int TCOLS = COLS <= 32 ? 32 : (COLS <= 64 ? 64 : (COLS <= 128 ? 128 : 256));
+    static constexpr int KC = 32;                                  // cells per stage
+    static constexpr int ABLK = 4096;                              // 128 x 16 BF16
+    static constexpr int BBLK = COUT * 32;                         // COUT x 16 BF16
+    static constexpr int STAGE = G * 2 * ABLK + 2 * BBLK;
+    static constexpr int SMEM = 2 * STAGE;
+};
+
+template <int CIN, int COUT>
+__global__ void __launch_bounds__(kThreads) wgrad_kernel(Grid3 g, const __nv_bfloat16* __restrict__ act,
+                                                         const __nv_bfloat16* __restrict__ grad,
+                                                         float* __restrict__ partials, int* __restrict__ err) {
+    using WS = WGradShape<CIN, COUT>;
+    constexpr int TPG = WS::TPG, G = WS::G, KC = WS::KC;
+    extern __shared__ __align__(1024) unsigned char sm[];
+    __shared__ uint64_t bar[2];
+    __shared__ uint32_t tslot;
+    const int t = threadIdx.x;
+    if (t == 0) {
+        tc::mbar_init(&bar[0], 1);
+        tc::mbar_init(&bar[1], 1);
+        tc::mbar_fence_init();
+    }
+    if (t < 32) tc::tmem_alloc(&tslot, WS::TCOLS);
+    tc::fence_before_sync();
+    __syncthreads();
+    tc::fence_after_sync();
+    const uint32_t tmem = tslot;
+    const uint32_t idesc = tc::idesc_bf16(kTileM, COUT, 1, 1);
+    const uint32_t s0 = tc::smem_addr(sm);
+    uint32_t uses[2] = {0, 0};
+    bool ok = true;
+
+    const int64_t nchunks = (g.V + KC - 1) / KC;
+    const int64_t ch0 = nchunks * blockIdx.x / gridDim.x, ch1 = nchunks * (blockIdx.x + 1) / gridDim.x;
+    bool first = true;
+    for (int64_t ch = ch0; ch < ch1; ++ch) {
+        const int s = (int)((ch - ch0) & 1);
+        bool lost = uses[s] > 0 && !tc::mbar_wait(&bar[s], (uses[s] - 1) & 1, err);
+        if (__syncthreads_or(lost)) {
+            ok = false;
+            break;
+        }
+        unsigned char* st = sm + s * WS::STAGE;
+        // A: item = (slot = tap slot of 28 or 32, q = ci chunk of 8, k = cell of KC)
+        constexpr int NA = G * TPG * (CIN / 8) * KC;
+        for (int i = t; i < NA; i += kThreads) {
+            const int q = i % (CIN / 8);
+            const int k = (i / (CIN / 8)) % KC;
+            const int slot = i / ((CIN / 8) * KC);
+            const int gi = slot / TPG, j = slot % TPG;
+            const int64_t c = ch * KC + k;
+            uint4 v = make_uint4(0, 0, 0, 0);
+            if (slot < 27 && c < g.V) {
+                const int x = (int)(c % g.nx), y = (int)((c / g.nx) % g.ny), z = (int)(c / ((int64_t)g.nx * g.ny));
+                v = reinterpret_cast<const uint4*>(act + neighbour(g, x, y, z, slot) * CIN)[q];
+            }
+            const int m = j * CIN + q * 8;
+            const int kk = k % 16;
+            *reinterpret_cast<uint4*>(st + (gi * 2 + k / 16) * WS::ABLK + (m / 8) * 128 + (kk / 8) * 2048 +
+                                      (kk % 8) * 16) = v;
+        }
+        // B: item = (q = co chunk of 8, k)
+        unsigned char* bst = st + G * 2 * WS::ABLK;
+        for (int i = t; i < (COUT / 8) * KC; i += kThreads) {
+            const int q = i % (COUT / 8), k = i / (COUT / 8);
+            const int64_t c = ch * KC + k;
+            uint4 v = make_uint4(0, 0, 0, 0);
+            if (c < g.V) v = reinterpret_cast<const uint4*>(grad + c * COUT)[q];
+            const int kk = k % 16;
+            *reinterpret_cast<uint4*>(bst + (k / 16) * WS::BBLK + q * 128 + (kk / 8) * (COUT / 8) * 128 +
+                                      (kk % 8) * 16) = v;
+        }
+        tc::fence_smem_async();
+        tc::fence_before_sync();
+        __syncthreads();
+        tc::fence_after_sync();
+        if (t == 0) {
+            const uint32_t sa = s0 + s * WS::STAGE;
+#pragma unroll 1
+            for (int gi = 0; gi < G; ++gi) {
+#pragma unroll
+                for (int ks = 0; ks < 2; ++ks) {
+                    const uint64_t da = tc::smem_desc(sa + (gi * 2 + ks) * WS::ABLK, 2048, 128);
+                    const uint64_t db = tc::smem_desc(sa + G * 2 * WS::ABLK + ks * WS::BBLK, (COUT / 8) * 128, 128);
+                    tc::mma_bf16(tmem + gi * COUT, da, db, idesc, (first && ks == 0) ? 0u : 1u);
+                }
+            }
+            tc::mma_commit(&bar[s]);
+        }
+        first = false;
+        ++uses[s];
+    }
+    if (ok && uses[0] + uses[1] > 0) {
+        const int last = (int)(((ch1 - ch0) - 1) & 1);
+        const bool lost = !tc::mbar_wait(&bar[last], (uses[last] - 1) & 1, err);
+        ok = !__syncthreads_or(lost);
+    }
+    tc::fence_after_sync();
+    if (ok) {
+        const int w = t >> 5;
+        const int j = t / CIN, ci = t % CIN;
+        float* dst = partials + (int64_t)blockIdx.x * 27 * CIN * COUT;
+        for (int gi = 0; gi < G; ++gi) {
+            float v[COUT];
+            if (first) {
+#pragma unroll
+                for (int co = 0; co < COUT; ++co) v[co] = 0.0f;  // no cells: zero partial
+            } else {
+#pragma unroll
+                for (int c0 = 0; c0 < COUT; c0 += 16)
+                    tc::tmem_ld16(tmem + ((uint32_t)(32 * w) << 16) + (uint32_t)(gi * COUT + c0), v + c0);
+            }
+            const int tap = gi * TPG + j;
+            if (tap < 27) {
+#pragma unroll
+                for (int co = 0; co < COUT; ++co) dst[((int64_t)tap * CIN + ci) * COUT + co] = v[co];
+            }
+        }
+    }
+    if (t == 0) {
+        for (int s = 0; s < 2; ++s)
+            if (uses[s] > 0) tc::mbar_wait(&bar[s], (uses[s] - 1) & 1, err);
+    }
+    tc::fence_before_sync();
+    __syncthreads();
+    if (t < 32) tc::tmem_dealloc(tmem, WS::TCOLS);
+}
+
+// out[j] = sum over p < P (in order) of partials[p * n + j].
+__global__ void sum_partials_kernel(const float* __restrict__ partials, int P, int n, float* __restrict__ out) {
+    const int j = blockIdx.x * blockDim.x + threadIdx.x;
+    if (j >= n) return;
+    float acc = 0.0f;
+    for (int p = 0; p < P; ++p) acc += partials[(int64_t)p * n + j];
+    out[j] = acc;
+}
+
+// Bias gradient partials: per block, sum over its cells of grad[c][co].
+template <int C>
+__global__ void bias_grad_kernel(const __nv_bfloat16* __restrict__ grad, int64_t V, float* __restrict__ partials) {
+    __shared__ float sh[kThreads / 32][C];
+    float acc[C];
+#pragma unroll
+    for (int j = 0; j < C; ++j) acc[j] = 0.0f;
+    for (int64_t c = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; c < V; c += (int64_t)gridDim.x * blockDim.x) {
+#pragma unroll
+        for (int j = 0; j < C; ++j) acc[j] += __bfloat162float(grad[c * C + j]);
+    }
+#pragma unroll
+    for (int j = 0; j < C; ++j) {
+        float v = acc[j];
+        for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
+        if ((threadIdx.x & 31) == 0) sh[threadIdx.x >> 5][j] = v;
+    }
+    __syncthreads();
+    if (threadIdx.x < C) {
+        float v = 0.0f;
+        for (int w = 0; w < kThreads / 32; ++w) v += sh[w][threadIdx.x];
+        partials[(int64_t)blockIdx.x * C + threadIdx.x] = v;
+    }
+}
+
+// Fwd and backward-data B images of one layer from the FP32 master weights
+// W[27][CIN][COUT] (padding rows/columns are zero in the master copy).
+template <int CIN, int COUT>
+__global__ void pack_kernel(const float* __restrict__ W, __nv_bfloat16* __restrict__ fwd,
+                            __nv_bfloat16* __restrict__ bwd) {
+    const int n = 27 * CIN * COUT;
+    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+        const int co = i % COUT, ci = (i / COUT) % CIN, tap = i / (CIN * COUT);
+        const __nv_bfloat16 v = __float2bfloat16(W[i]);
+        {  // forward: B[n = co][k = ci] of k-step (tap, ci/16)
+            const int s = tap * (CIN / 16) + ci / 16, k = ci % 16;
+            fwd[(s * COUT * 32 + tc::kmajor_off(co, k, 128, 256)) / 2] = v;
+        }
+        if (bwd) {  // backward data: tap' = 26 - tap, B[n = ci][k = co]
+            const int tp = 26 - tap;
+            const int s = tp * (COUT / 16) + co / 16, k = co % 16;
+            bwd[(s * CIN * 32 + tc::kmajor_off(ci, k, 128, 256)) / 2] = v;
+        }
+    }
+}
+
+// Adam on the flat FP32 parameter vector.
+__global__ void adam_kernel(float* __restrict__ p, const float* __restrict__ grad, float* __restrict__ m,
+                            float* __restrict__ v, const float* __restrict__ mask, int n, float lr, float b1,
+                            float b2, float eps, float bc1, float bc2) {
+    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+        const float gi = grad[i] * mask[i];
+        const float mi = b1 * m[i] + (1.0f - b1) * gi;
+        const float vi = b2 * v[i] + (1.0f - b2) * gi * gi;
+        m[i] = mi;
+        v[i] = vi;
+        p[i] -= mask[i] * lr * (mi / bc1) / (sqrtf(vi / bc2) + eps);
+    }
+}
+
+// Network input from 9 FP32 channel blocks (rho, u, Q; [9][V]):
+// act0[c][j] = (x_j - shift_j) * inv_scale_j for j < 9, 0 for j in 9..15.
+__global__ void features_kernel(const float* __restrict__ rho, const float* __restrict__ u3,
+                                const float* __restrict__ q5, int64_t V, const float* __restrict__ shift,
+                                const float* __restrict__ inv_scale, __nv_bfloat16* __restrict__ act0) {
+    for (int64_t c = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; c < V; c += (int64_t)gridDim.x * blockDim.x) {
+        __align__(16) __nv_bfloat16 v[16];
+        float x[9];
+        x[0] = rho[c];
+#pragma unroll
+        for (int k = 0; k < 3; ++k) x[1 + k] = u3[k * V + c];
+#pragma unroll
+        for (int k = 0; k < 5; ++k) x[4 + k] = q5[k * V + c];
+#pragma unroll
+        for (int j = 0; j < 16; ++j) v[j] = __float2bfloat16(j < 9 ? (x[j] - shift[j]) * inv_scale[j] : 0.0f);
+        reinterpret_cast<uint4*>(act0 + c * 16)[0] = reinterpret_cast<const uint4*>(v)[0];
+        reinterpret_cast<uint4*>(act0 + c * 16)[1] = reinterpret_cast<const uint4*>(v)[1];
+    }
+}
+
+// Mean-squared error of the 8 outputs against the raw targets [8][V]
+// normalised by inv_scale, its gradient gout[c][16] (BF16, channels 8..15
+// zero) and per-block partial sums of the squared error.
+__global__ void __launch_bounds__(kThreads) loss_kernel(const float* __restrict__ out, const float* __restrict__ tgt,
+                                                        const float* __restrict__ inv_scale, int64_t V,
+                                                        __nv_bfloat16* __restrict__ gout,
+                                                        double* __restrict__ partials) {
+    __shared__ double sh[kThreads / 32];
+    double acc = 0.0;
+    const float gscale = 2.0f / (8.0f * (float)V);
+    for (int64_t c = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; c < V; c += (int64_t)gridDim.x * blockDim.x) {
+        __align__(16) __nv_bfloat16 gv[16];
+#pragma unroll
+        for (int j = 0; j < 16; ++j) {
+            float gj = 0.0f;
+            if (j < 8) {
+                const float d = out[c * 16 + j] - tgt[j * V + c] * inv_scale[j];
+                acc += (double)d * d;
+                gj = gscale * d;
+            }
+            gv[j] = __float2bfloat16(gj);
+        }
+        reinterpret_cast<uint4*>(gout + c * 16)[0] = reinterpret_cast<const uint4*>(gv)[0];
+        reinterpret_cast<uint4*>(gout + c * 16)[1] = reinterpret_cast<const uint4*>(gv)[1];
+    }
+    for (int o = 16; o > 0; o >>= 1) acc += __shfl_xor_sync(0xffffffffu, acc, o);
+    if ((threadIdx.x & 31) == 0) sh[threadIdx.x >> 5] = acc;
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        double v = 0.0;
+        for (int w = 0; w < kThreads / 32; ++w) v += sh[w];
+        partials[blockIdx.x] = v;
+    }
+}
+
+// Correction of a coarse state after its step: Q_k += out[c][k] * s_k
+// (k < 5), u_d += out[c][5+d] * s_{5+d}.
+__global__ void apply_kernel(const float* __restrict__ out, const float* __restrict__ out_scale, int64_t V,
+                             float* __restrict__ u3, float* __restrict__ q5) {
+    for (int64_t c = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; c < V; c += (int64_t)gridDim.x * blockDim.x) {
+#pragma unroll
+        for (int k = 0; k < 5; ++k) q5[k * V + c] += out[c * 16 + k] * out_scale[k];
+#pragma unroll
+        for (int d = 0; d < 3; ++d) u3[d * V + c] += out[c * 16 + 5 + d] * out_scale[5 + d];
+    }
+}
+
+// Box filter of a fine state (factor f per axis) onto the coarse grid:
+// rho_c = <rho>, u_c = <rho u> / rho_c, Q_c = <Q>; out [9][Vc].
+__global__ void filter_kernel(const float* __restrict__ rho, const float* __restrict__ u3,
+                              const float* __restrict__ q5, int nx, int ny, int nz, int f,
+                              float* __restrict__ out) {
+    const int cx = nx / f, cy = ny / f, cz = nz / f;
+    const int64_t Vc = (int64_t)cx * cy * cz, V = (int64_t)nx * ny * nz;
+    const double inv = 1.0 / ((double)f * f * f);
+    for (int64_t c = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; c < Vc; c += (int64_t)gridDim.x * blockDim.x) {
+        const int X = (int)(c % cx), Y = (int)((c / cx) % cy), Z = (int)(c / ((int64_t)cx * cy));
+        double r = 0, m[3] = {0, 0, 0}, q[5] = {0, 0, 0, 0, 0};
+        for (int dz = 0; dz < f; ++dz)
+            for (int dy = 0; dy < f; ++dy)
+                for (int dx = 0; dx < f; ++dx) {
+                    const int64_t i = ((int64_t)(Z * f + dz) * ny + (Y * f + dy)) * nx + (X * f + dx);
+                    const double ri = rho[i];
+                    r += ri;
+#pragma unroll
+                    for (int d = 0; d < 3; ++d) m[d] += ri * u3[d * V + i];
+#pragma unroll
+                    for (int k = 0; k < 5; ++k) q[k] += q5[k * V + i];
+                }
+        out[c] = (float)(r * inv);
+#pragma unroll
+        for (int d = 0; d < 3; ++d) out[(1 + d) * Vc + c] = (float)(m[d] / r);
+#pragma unroll
+        for (int k = 0; k < 5; ++k) out[(4 + k) * Vc + c] = (float)(q[k] * inv);
+    }
+}
+
+// Per-block sums and sums of squares of nc channel blocks [nc][V] (or a
+// difference a - b when b is given): partials[(blk * nc + j) * 2 + {0,1}].
+__global__ void __launch_bounds__(kThreads) moments_kernel(const float* __restrict__ a, const float* __restrict__ b,
+                                                           int nc, int64_t V, double* __restrict__ partials) {
+    __shared__ double sh[2][kThreads / 32];
+    for (int j = 0; j < nc; ++j) {
+        double s1 = 0.0, s2 = 0.0;
+        for (int64_t c = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; c < V;
+             c += (int64_t)gridDim.x * blockDim.x) {
+            const double x = (double)a[j * V + c] - (b ? (double)b[j * V + c] : 0.0);
+            s1 += x;
+            s2 += x * x;
+        }
+        for (int o = 16; o > 0; o >>= 1) {
+            s1 += __shfl_xor_sync(0xffffffffu, s1, o);
+            s2 += __shfl_xor_sync(0xffffffffu, s2, o);
+        }
+        if ((threadIdx.x & 31) == 0) {
+            sh[0][threadIdx.x >> 5] = s1;
+            sh[1][threadIdx.x >> 5] = s2;
+        }
+        __syncthreads();
+        if (threadIdx.x == 0) {
+            double v1 = 0.0, v2 = 0.0;
+            for (int w = 0; w < kThreads / 32; ++w) {
+                v1 += sh[0][w];
+                v2 += sh[1][w];
+            }
+            partials[((int64_t)blockIdx.x * nc + j) * 2] = v1;
+            partials[((int64_t)blockIdx.x * nc + j) * 2 + 1] = v2;
+        }
+        __syncthreads();
+    }
+}
+
+// Raw training target [8][V]: next - pred, Q components then u.
+__global__ void target_kernel(const float* __restrict__ next9, const float* __restrict__ pu3,
+                              const float* __restrict__ pq5, int64_t V, float* __restrict__ tgt) {
+    for (int64_t c = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; c < V; c += (int64_t)gridDim.x * blockDim.x) {
+#pragma unroll
+        for (int k = 0; k < 5; ++k) tgt[k * V + c] = next9[(4 + k) * V + c] - pq5[k * V + c];
+#pragma unroll
+        for (int d = 0; d < 3; ++d) tgt[(5 + d) * V + c] = next9[(1 + d) * V + c] - pu3[d * V + c];
+    }
+}
+
+}  // namespace cl
+}  // namespace lbman

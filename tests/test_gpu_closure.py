@@ -1,0 +1,82 @@
+"""The learned closure on the GPU: the tcgen05 self-test, forward and
+gradient against the FP64 oracle network (oracle/closure.py) with BF16
+emulation, and the record -> targets -> train -> corrected-run pipeline.
+Parity for this row is unpinned by the reference (it has no closure).
+"""
+import numpy as np
+import pytest
+
+import lbman3d_b200 as L
+from lbman3d_b200 import closure as CL
+from oracle import closure as K
+
+pytestmark = pytest.mark.gpu
+
+
+def _case(grid, seed):
+    nx, ny, nz = grid
+    V = nx * ny * nz
+    r = np.random.default_rng(seed)
+    feat = r.standard_normal((9, V)).astype(np.float32)
+    feat[0] += 1.0
+    tgt = r.standard_normal((8, V)).astype(np.float32)
+    return feat, tgt
+
+
+def test_tensor_core_selftest():
+    e = np.zeros(4)
+    L._native.check(L._native.lib().lbman_closure_selftest(0, L._native.dptr(e)))
+    assert np.all(e >= 0) and np.all(e < 1e-6), e
+
+
+@pytest.mark.parametrize("grid", [(8, 8, 8), (5, 6, 7), (16, 8, 4)])
+def test_forward_matches_oracle(grid):
+    feat, _ = _case(grid, 1)
+    with CL.Closure(*grid, seed=5) as cl:
+        p = cl.params()
+        sh, sc, _ = cl.scales()
+        got = cl.forward(feat)
+    ref, _ = K.forward(feat, grid, p, sh, sc, bf=True)
+    ref = ref[..., :8].reshape(-1, 8).T
+    assert np.max(np.abs(got - ref)) <= 2e-2 * np.max(np.abs(ref))
+
+
+@pytest.mark.parametrize("grid", [(8, 8, 8), (5, 6, 7)])
+def test_gradient_matches_oracle(grid):
+    feat, tgt = _case(grid, 2)
+    with CL.Closure(*grid, seed=6) as cl:
+        p = cl.params()
+        sh, sc, osc = cl.scales()
+        loss, g = cl.gradient(feat, tgt)
+    lref, gref = K.loss_and_grad(feat, tgt, grid, p, sh, sc, osc, bf=True)
+    assert abs(loss - lref) <= 1e-3 * lref
+    for (w0, b0), (cin, cout) in zip(K.OFFSETS, K.LAYERS):
+        for a, b in ((w0, b0), (b0, b0 + cout)):
+            x, y = g[a:b].astype(np.float64), gref[a:b]
+            rel = np.linalg.norm(x - y) / max(np.linalg.norm(y), 1e-30)
+            cos = x @ y / max(np.linalg.norm(x) * np.linalg.norm(y), 1e-30)
+            assert rel <= 3e-2 and cos >= 0.999, (a, b, rel, cos)
+
+
+def test_pipeline_trains_and_runs():
+    fine_p = L.Params(nx=32, ny=32, nz=32, ALPHA=0.01)
+    coarse_p = CL.coarse_params(fine_p, 4)
+    assert coarse_p.nx == 8 and abs(coarse_p.TAUF - 1.0) < 1e-12
+    with L.Simulation(fine_p, L.FullyPeriodicConfig(), L.Precision.FP32) as fine, \
+            L.Simulation(coarse_p, L.FullyPeriodicConfig(), L.Precision.FP32) as coarse, \
+            CL.Closure(8, 8, 8, seed=1) as cl:
+        fine.init_seeded(3, 0.5, 1e-3)
+        fine.step(40)
+        cl.record(fine, new_trajectory=True)
+        for _ in range(12):
+            fine.step(4)
+            cl.record(fine)
+        assert cl.dataset() == (13, 0)
+        cl.build_targets(coarse)
+        assert cl.dataset() == (13, 12)
+        first, last = cl.train(300, lr=1e-3, seed=2)
+        assert last < 0.7 * first, (first, last)
+        cl.load_snapshot(0, coarse)
+        cl.step(coarse, 3)
+        out = coarse.download()
+        assert np.all(np.isfinite(out["q"])) and np.all(np.isfinite(out["u"]))
