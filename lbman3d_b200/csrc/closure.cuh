@@ -29,6 +29,7 @@ namespace cl {
 
 constexpr int kTileM = 128;
 constexpr int kThreads = 128;
+constexpr int kStages = 4;  // A-operand stages of the convolution pipeline
 
 struct Grid3 {
     int nx, ny, nz;
@@ -59,29 +60,45 @@ enum ConvMode : int {
     kBwdData = 2     // times GELU'(pre of the layer below), store BF16
 };
 
-// One persistent CTA walks 128-cell tiles.  Smem: B image, then 2 A stages
-// of CIN/16 x 4 KB.
+// Halo staging applies when a 128-cell tile is R = 128/nx whole x rows of
+// one z plane: then the tile's input neighbourhood (3 planes x R+2 rows x nx
+// cells) is copied into shared memory once per tile and the 27 tap operands
+// are built from it, instead of 27 gathers from L2.
+__host__ __device__ inline bool halo_ok(int nx, int ny) {
+    return nx <= kTileM && kTileM % nx == 0 && ((int64_t)nx * ny) % kTileM == 0;
+}
+__host__ __device__ inline int halo_bytes(int nx, int cin) { return 3 * (kTileM / nx + 2) * nx * cin * 2; }
+
+// One persistent CTA walks 128-cell tiles.  Smem: B image, kStages A stages
+// of CIN/16 x 4 KB, then (halo != 0) the staged neighbourhood.  The operand
+// of tap k goes to stage k % kStages once the MMAs that last read that stage
+// have completed, so operand copies run up to kStages - 1 taps ahead of the
+// tensor core.  Halo units of
+// 16 bytes are stored at cell * (CIN/8) + (q ^ (cell & (CIN/8 - 1))), an XOR
+// swizzle that spreads a warp's reads of one q over the banks.
 template <int CIN, int COUT, int MODE>
 __global__ void __launch_bounds__(kThreads) conv_kernel(Grid3 g, const __nv_bfloat16* __restrict__ in,
                                                         const uint4* __restrict__ bimg, const float* __restrict__ bias,
                                                         const __nv_bfloat16* __restrict__ pre_below,
                                                         __nv_bfloat16* __restrict__ out_pre,
                                                         __nv_bfloat16* __restrict__ out_bf, float* __restrict__ out_f,
-                                                        int* __restrict__ err) {
+                                                        int halo, int* __restrict__ err) {
     constexpr int KS = CIN / 16;                 // k-steps per tap
     constexpr int BBYTES = bimg_bytes(CIN, COUT);
     constexpr int ABYTES = KS * 4096;            // one A stage
     extern __shared__ __align__(1024) unsigned char sm[];
-    __shared__ uint64_t bar[2];
+    __shared__ uint64_t bar[kStages];
     __shared__ uint32_t tslot;
+    constexpr int QU = CIN / 8;                  // 16-byte units per cell
     unsigned char* Bs = sm;
     unsigned char* As = sm + BBYTES;
+    uint4* Hs = reinterpret_cast<uint4*>(sm + BBYTES + kStages * ABYTES);
     const int t = threadIdx.x;
+    const int R = kTileM / g.nx;                 // rows per tile (halo path)
 
     for (int i = t; i < BBYTES / 16; i += kThreads) reinterpret_cast<uint4*>(Bs)[i] = bimg[i];
     if (t == 0) {
-        tc::mbar_init(&bar[0], 1);
-        tc::mbar_init(&bar[1], 1);
+        for (int k = 0; k < kStages; ++k) tc::mbar_init(&bar[k], 1);
         tc::mbar_fence_init();
     }
     if (t < 32) tc::tmem_alloc(&tslot, 32);
@@ -92,7 +109,9 @@ __global__ void __launch_bounds__(kThreads) conv_kernel(Grid3 g, const __nv_bflo
     const uint32_t tmem = tslot;
     const uint32_t idesc = tc::idesc_bf16(kTileM, COUT, 0, 0);
     const uint32_t a0 = tc::smem_addr(As), b0 = tc::smem_addr(Bs);
-    uint32_t uses[2] = {0, 0};  // commits issued per A stage (same in every thread)
+    uint32_t uses[kStages] = {};  // commits issued per A stage (same in every thread)
+    int kt = 0;                     // taps issued so far by this CTA
+    int last_s = 0;
     bool ok = true;
 
     const int64_t ntiles = (g.V + kTileM - 1) / kTileM;
@@ -101,20 +120,47 @@ __global__ void __launch_bounds__(kThreads) conv_kernel(Grid3 g, const __nv_bflo
         const bool live = c < g.V;
         const int64_t cc = live ? c : 0;
         const int x = (int)(cc % g.nx), y = (int)((cc / g.nx) % g.ny), z = (int)(cc / ((int64_t)g.nx * g.ny));
-        for (int tap = 0; tap < 27; ++tap) {
-            const int s = tap & 1;
+        if (halo) {
+            // planes z0-1..z0+1, rows y0-1..y0+R of the tile's plane
+            const int64_t c0 = tile * kTileM;
+            const int z0 = (int)(c0 / ((int64_t)g.nx * g.ny)), y0 = (int)((c0 / g.nx) % g.ny);
+            const int nunits = 3 * (R + 2) * g.nx * QU;
+            for (int i = t; i < nunits; i += kThreads) {
+                const int q = i % QU, cell = i / QU;
+                const int hx = cell % g.nx, hr = (cell / g.nx) % (R + 2), hz = cell / (g.nx * (R + 2));
+                const int64_t src = ((int64_t)wrapi(z0 - 1 + hz, g.nz) * g.ny + wrapi(y0 - 1 + hr, g.ny)) * g.nx + hx;
+                const uint4* gp = reinterpret_cast<const uint4*>(in + src * CIN) + q;
+                asm volatile("cp.async.cg.shared.global [%0], [%1], 16;\n" ::"r"(
+                                 tc::smem_addr(Hs + cell * QU + (q ^ (cell & (QU - 1))))),
+                             "l"(gp));
+            }
+            asm volatile("cp.async.wait_all;\n" ::: "memory");
+            __syncthreads();
+        }
+        for (int tap = 0; tap < 27; ++tap, ++kt) {
+            const int s = kt % kStages;
             // stage s is free once the MMAs that read it last have completed
             bool lost = uses[s] > 0 && !tc::mbar_wait(&bar[s], (uses[s] - 1) & 1, err);
             if (__syncthreads_or(lost)) {
                 ok = false;
                 break;
             }
-            // gather this row's CIN channels of the neighbour into stage s
-            const uint4* src = reinterpret_cast<const uint4*>(in + neighbour(g, x, y, z, tap) * CIN);
+            // this row's CIN channels of the neighbour into stage s
             unsigned char* dst = As + s * ABYTES + (t / 8) * 256 + (t % 8) * 16;
+            if (halo) {
+                const int dx = tap % 3 - 1, dy = (tap / 3) % 3 - 1, dz = tap / 9 - 1;
+                const int hx = wrapi(t % g.nx + dx, g.nx), hr = t / g.nx + 1 + dy;
+                const int cell = ((1 + dz) * (R + 2) + hr) * g.nx + hx;
 #pragma unroll
-            for (int q = 0; q < CIN / 8; ++q)
-                *reinterpret_cast<uint4*>(dst + (q / 2) * 4096 + (q % 2) * 128) = src[q];
+                for (int q = 0; q < QU; ++q)
+                    *reinterpret_cast<uint4*>(dst + (q / 2) * 4096 + (q % 2) * 128) =
+                        Hs[cell * QU + (q ^ (cell & (QU - 1)))];
+            } else {
+                const uint4* src = reinterpret_cast<const uint4*>(in + neighbour(g, x, y, z, tap) * CIN);
+#pragma unroll
+                for (int q = 0; q < QU; ++q)
+                    *reinterpret_cast<uint4*>(dst + (q / 2) * 4096 + (q % 2) * 128) = src[q];
+            }
             tc::fence_smem_async();
             tc::fence_before_sync();
             __syncthreads();
@@ -129,10 +175,11 @@ __global__ void __launch_bounds__(kThreads) conv_kernel(Grid3 g, const __nv_bflo
                 tc::mma_commit(&bar[s]);
             }
             ++uses[s];
+            last_s = s;
         }
         if (!ok) break;
-        // the last commit (tap 26, stage 0) covers every MMA of the tile
-        const bool lost = !tc::mbar_wait(&bar[0], (uses[0] - 1) & 1, err);
+        // the tile's last commit covers every MMA issued before it
+        const bool lost = !tc::mbar_wait(&bar[last_s], (uses[last_s] - 1) & 1, err);
         if (__syncthreads_or(lost)) {
             ok = false;
             break;
@@ -180,12 +227,200 @@ __global__ void __launch_bounds__(kThreads) conv_kernel(Grid3 g, const __nv_bflo
     }
     // drain: never leave with MMAs in flight on our TMEM
     if (t == 0) {
-        for (int s = 0; s < 2; ++s)
+        for (int s = 0; s < kStages; ++s)
             if (uses[s] > 0) tc::mbar_wait(&bar[s], (uses[s] - 1) & 1, err);
     }
     tc::fence_before_sync();
     __syncthreads();
     if (t < 32) tc::tmem_dealloc(tmem, 32);
+}
+
+// ---- descriptor-halo convolution -------------------------------------------
+// Tile = 8 x-cells by 16 y-rows of one z plane (128 cells, M row m = 8*dy_row
+// + dx_cell).  The tile's neighbourhood (10 x 18 x 3 cells) is staged once
+// as 16-byte units, one plane per 8-channel group:
+//   unit(kg, hz, hy, hx) at ((kg*3 + hz)*18 + hy)*10 + hx,
+// which makes the A operand of every tap a K-major view of the halo: rows
+// of a core matrix are 8 consecutive x cells (16 bytes apart), the next
+// y row is SBO = 160 bytes on, the next 8 channels LBO = 8640 bytes on, and
+// the tap shift (dx, dy, dz) only moves the start address.  So each tile is
+// one halo copy and 27 x CIN/16 back-to-back MMAs with no operand copies;
+// the halo and the TMEM accumulator are double-buffered so the next tile's
+// copy and this tile's epilogue overlap the tensor core.
+constexpr int kHX = 10, kHY = 18, kHZ = 3;
+constexpr int kHaloPlane = kHX * kHY * kHZ * 16;  // bytes per 8-channel group
+
+__host__ __device__ inline bool dhalo_ok(int nx, int ny) { return nx % 8 == 0 && ny % 16 == 0; }
+__host__ __device__ constexpr int dhalo_bytes(int cin) { return (cin / 8) * kHaloPlane; }
+
+template <int CIN>
+__device__ __forceinline__ void dhalo_load(const Grid3& g, const __nv_bfloat16* __restrict__ in, int x0, int y0,
+                                           int z0, unsigned char* H) {
+    constexpr int QU = CIN / 8;
+    constexpr int N = QU * kHX * kHY * kHZ;
+    for (int i = threadIdx.x; i < N; i += kThreads) {
+        const int hx = i % kHX, hy = (i / kHX) % kHY, hz = (i / (kHX * kHY)) % kHZ, kg = i / (kHX * kHY * kHZ);
+        const int64_t cell =
+            ((int64_t)wrapi(z0 - 1 + hz, g.nz) * g.ny + wrapi(y0 - 1 + hy, g.ny)) * g.nx + wrapi(x0 - 1 + hx, g.nx);
+        const uint4* src = reinterpret_cast<const uint4*>(in + cell * CIN) + kg;
+        asm volatile("cp.async.cg.shared.global [%0], [%1], 16;\n" ::"r"(tc::smem_addr(H + i * 16)), "l"(src));
+    }
+}
+
+template <int COUT, int MODE>
+__device__ __forceinline__ void conv_epilogue(uint32_t tacc, int64_t c, const float* __restrict__ bias,
+                                              const __nv_bfloat16* __restrict__ pre_below,
+                                              __nv_bfloat16* __restrict__ out_pre, __nv_bfloat16* __restrict__ out_bf,
+                                              float* __restrict__ out_f) {
+    const int w = threadIdx.x >> 5;
+    float acc[COUT];
+#pragma unroll
+    for (int c0 = 0; c0 < COUT; c0 += 16) tc::tmem_ld16(tacc + ((uint32_t)(32 * w) << 16) + (uint32_t)c0, acc + c0);
+    if constexpr (MODE == kFwdHidden) {
+        __align__(16) __nv_bfloat16 pb[COUT], ab[COUT];
+#pragma unroll
+        for (int j = 0; j < COUT; ++j) {
+            const float p = acc[j] + bias[j];
+            pb[j] = __float2bfloat16(p);
+            ab[j] = __float2bfloat16(gelu(p));
+        }
+#pragma unroll
+        for (int q = 0; q < COUT / 8; ++q) {
+            reinterpret_cast<uint4*>(out_pre + c * COUT)[q] = reinterpret_cast<const uint4*>(pb)[q];
+            reinterpret_cast<uint4*>(out_bf + c * COUT)[q] = reinterpret_cast<const uint4*>(ab)[q];
+        }
+    } else if constexpr (MODE == kFwdLast) {
+#pragma unroll
+        for (int j = 0; j < COUT; j += 4)
+            reinterpret_cast<float4*>(out_f + c * COUT)[j / 4] = make_float4(
+                acc[j] + bias[j], acc[j + 1] + bias[j + 1], acc[j + 2] + bias[j + 2], acc[j + 3] + bias[j + 3]);
+    } else {
+        __align__(16) __nv_bfloat16 pre[COUT], gb[COUT];
+#pragma unroll
+        for (int q = 0; q < COUT / 8; ++q)
+            reinterpret_cast<uint4*>(pre)[q] = reinterpret_cast<const uint4*>(pre_below + c * COUT)[q];
+#pragma unroll
+        for (int j = 0; j < COUT; ++j) gb[j] = __float2bfloat16(acc[j] * gelu_grad(__bfloat162float(pre[j])));
+#pragma unroll
+        for (int q = 0; q < COUT / 8; ++q)
+            reinterpret_cast<uint4*>(out_bf + c * COUT)[q] = reinterpret_cast<const uint4*>(gb)[q];
+    }
+}
+
+// Smem: B image, then two halo buffers.  TMEM: two 32-column accumulators.
+template <int CIN, int COUT, int MODE>
+__global__ void __launch_bounds__(kThreads) conv_dhalo_kernel(Grid3 g, const __nv_bfloat16* __restrict__ in,
+                                                              const uint4* __restrict__ bimg,
+                                                              const float* __restrict__ bias,
+                                                              const __nv_bfloat16* __restrict__ pre_below,
+                                                              __nv_bfloat16* __restrict__ out_pre,
+                                                              __nv_bfloat16* __restrict__ out_bf,
+                                                              float* __restrict__ out_f, int* __restrict__ err) {
+    constexpr int KS = CIN / 16;
+    constexpr int BBYTES = bimg_bytes(CIN, COUT);
+    constexpr int HB = dhalo_bytes(CIN);
+    extern __shared__ __align__(1024) unsigned char sm[];
+    __shared__ uint64_t bar[2];
+    __shared__ uint32_t tslot;
+    unsigned char* Bs = sm;
+    unsigned char* Hs = sm + BBYTES;
+    const int t = threadIdx.x;
+    for (int i = t; i < BBYTES / 16; i += kThreads) reinterpret_cast<uint4*>(Bs)[i] = bimg[i];
+    if (t == 0) {
+        tc::mbar_init(&bar[0], 1);
+        tc::mbar_init(&bar[1], 1);
+        tc::mbar_fence_init();
+    }
+    if (t < 32) tc::tmem_alloc(&tslot, 64);
+    const int bx = g.nx / 8, by = g.ny / 16;
+    const int64_t ntiles = (int64_t)bx * by * g.nz;
+    auto origin = [&](int64_t tile, int& x0, int& y0, int& z0) {
+        x0 = (int)(tile % bx) * 8;
+        y0 = (int)((tile / bx) % by) * 16;
+        z0 = (int)(tile / ((int64_t)bx * by));
+    };
+    int x0, y0, z0;
+    if (blockIdx.x < ntiles) {
+        origin(blockIdx.x, x0, y0, z0);
+        dhalo_load<CIN>(g, in, x0, y0, z0, Hs);
+    }
+    asm volatile("cp.async.wait_all;\n" ::: "memory");
+    tc::fence_smem_async();
+    tc::fence_before_sync();
+    __syncthreads();
+    tc::fence_after_sync();
+    const uint32_t tmem = tslot;
+    const uint32_t idesc = tc::idesc_bf16(kTileM, COUT, 0, 0);
+    const uint32_t h0 = tc::smem_addr(Hs), b0 = tc::smem_addr(Bs);
+    uint32_t uses[2] = {0, 0};
+    bool ok = true;
+    int64_t prev = -1;  // tile whose epilogue is pending
+    int n = 0;
+    for (int64_t tile = blockIdx.x; tile < ntiles && ok; tile += gridDim.x, ++n) {
+        const int b = n & 1;
+        if (t == 0) {
+            // the start address is the descriptor's low field (16-byte units,
+            // smem < 256 KB so no carry): tap offsets are added to it directly
+            const uint64_t da0 = tc::smem_desc(h0 + b * HB, kHaloPlane, kHX * 16);
+            const uint64_t db0 = tc::smem_desc(b0, 128, 256);
+#pragma unroll
+            for (int tap = 0; tap < 27; ++tap) {
+                const int dx = tap % 3 - 1, dy = (tap / 3) % 3 - 1, dz = tap / 9 - 1;
+#pragma unroll
+                for (int kb = 0; kb < KS; ++kb) {
+                    const uint32_t aoff = (uint32_t)((((2 * kb) * kHZ + 1 + dz) * kHY + 1 + dy) * kHX + 1 + dx);
+                    const uint32_t boff = (uint32_t)((tap * KS + kb) * COUT * 32 / 16);
+                    tc::mma_bf16(tmem + b * 32, da0 + aoff, db0 + boff, idesc, (tap > 0 || kb > 0) ? 1u : 0u);
+                }
+            }
+            tc::mma_commit(&bar[b]);
+        }
+        ++uses[b];
+        // stage the next tile's halo in the other buffer once the MMAs that
+        // read it (tile n-1) are done -- that wait also covers the pending epilogue
+        const int64_t next = tile + gridDim.x;
+        bool lost = uses[b ^ 1] > 0 && !tc::mbar_wait(&bar[b ^ 1], (uses[b ^ 1] - 1) & 1, err);
+        if (__syncthreads_or(lost)) {
+            ok = false;
+            break;
+        }
+        tc::fence_after_sync();
+        if (next < ntiles) {
+            int nx0, ny0, nz0;
+            origin(next, nx0, ny0, nz0);
+            dhalo_load<CIN>(g, in, nx0, ny0, nz0, Hs + (b ^ 1) * HB);
+        }
+        if (prev >= 0) {
+            int px, py, pz;
+            origin(prev, px, py, pz);
+            const int64_t c = ((int64_t)pz * g.ny + py + t / 8) * g.nx + px + t % 8;
+            conv_epilogue<COUT, MODE>(tmem + (b ^ 1) * 32, c, bias, pre_below, out_pre, out_bf, out_f);
+        }
+        asm volatile("cp.async.wait_all;\n" ::: "memory");
+        tc::fence_smem_async();
+        tc::fence_before_sync();
+        __syncthreads();  // next halo visible; accumulator b^1 read before its next MMAs
+        tc::fence_after_sync();
+        prev = tile;
+    }
+    if (ok && prev >= 0) {
+        const int b = (n - 1) & 1;
+        const bool lost = !tc::mbar_wait(&bar[b], (uses[b] - 1) & 1, err);
+        if (!__syncthreads_or(lost)) {
+            tc::fence_after_sync();
+            int px, py, pz;
+            origin(prev, px, py, pz);
+            const int64_t c = ((int64_t)pz * g.ny + py + t / 8) * g.nx + px + t % 8;
+            conv_epilogue<COUT, MODE>(tmem + b * 32, c, bias, pre_below, out_pre, out_bf, out_f);
+        }
+    }
+    if (t == 0) {
+        for (int s = 0; s < 2; ++s)
+            if (uses[s] > 0) tc::mbar_wait(&bar[s], (uses[s] - 1) & 1, err);
+    }
+    tc::fence_before_sync();
+    __syncthreads();
+    if (t < 32) tc::tmem_dealloc(tmem, 64);
 }
 
 // Weight gradient dW[tap][ci][co] = sum_c act[c + off(tap)][ci] * grad[c][co]
@@ -324,6 +559,147 @@ __global__ void __launch_bounds__(kThreads) wgrad_kernel(Grid3 g, const __nv_bfl
     tc::fence_before_sync();
     __syncthreads();
     if (t < 32) tc::tmem_dealloc(tmem, WS::TCOLS);
+}
+
+// Weight gradient on 8 x 16 x 1 tiles (nx % 8 == 0, ny % 16 == 0).  Per tile
+// the activation halo (same layout as conv_dhalo_kernel) and the tile's
+// output gradient are staged once; then for each group of TPG taps the
+// MN-major A operand (rows (tap, ci), K = the tile's 128 cells) is assembled
+// from the halo by 16-byte copies -- cell k of the tile is row k of every
+// 8-channel plane, so K-groups are 128 bytes apart and channel groups 2 KB --
+// and 8 K-steps of MMAs accumulate into the group's TMEM columns.  Two A
+// buffers let the copies of one group overlap the MMAs of the previous one.
+template <int CIN, int COUT>
+struct WGradHalo {
+    static constexpr int TPG = kTileM / CIN;
+    static constexpr int G = (27 + TPG - 1) / TPG;
+    static constexpr int TCOLS = WGradShape<CIN, COUT>::TCOLS;
+    static constexpr int HB = dhalo_bytes(CIN);
+    static constexpr int BB = (COUT / 8) * 2048;  // output-gradient tile
+    static constexpr int AB = 16 * 2048;          // one A buffer (128 x 128 BF16)
+    static constexpr int SMEM = HB + BB + 2 * AB;
+};
+
+template <int CIN, int COUT>
+__global__ void __launch_bounds__(kThreads) wgrad_dhalo_kernel(Grid3 g, const __nv_bfloat16* __restrict__ act,
+                                                               const __nv_bfloat16* __restrict__ grad,
+                                                               float* __restrict__ partials, int* __restrict__ err) {
+    using WH = WGradHalo<CIN, COUT>;
+    constexpr int TPG = WH::TPG, G = WH::G, QU = CIN / 8;
+    extern __shared__ __align__(1024) unsigned char sm[];
+    __shared__ uint64_t bar[2];
+    __shared__ uint32_t tslot;
+    unsigned char* Hs = sm;
+    unsigned char* Bs = sm + WH::HB;
+    unsigned char* As = Bs + WH::BB;
+    const int t = threadIdx.x;
+    if (t == 0) {
+        tc::mbar_init(&bar[0], 1);
+        tc::mbar_init(&bar[1], 1);
+        tc::mbar_fence_init();
+    }
+    if (t < 32) tc::tmem_alloc(&tslot, WH::TCOLS);
+    tc::fence_before_sync();
+    __syncthreads();
+    tc::fence_after_sync();
+    const uint32_t tmem = tslot;
+    const uint32_t idesc = tc::idesc_bf16(kTileM, COUT, 1, 1);
+    const uint32_t a0 = tc::smem_addr(As), b0 = tc::smem_addr(Bs);
+    const int bx = g.nx / 8, by = g.ny / 16;
+    const int64_t ntiles = (int64_t)bx * by * g.nz;
+    uint32_t uses[2] = {0, 0};
+    int kg_run = 0;  // groups issued so far (selects the A buffer)
+    int last_b = -1;
+    bool ok = true, any = false;
+    for (int64_t tile = blockIdx.x; tile < ntiles && ok; tile += gridDim.x) {
+        const int x0 = (int)(tile % bx) * 8, y0 = (int)((tile / bx) % by) * 16;
+        const int z0 = (int)(tile / ((int64_t)bx * by));
+        // the previous tile's MMAs read the gradient tile: let them finish
+        bool lost = last_b >= 0 && !tc::mbar_wait(&bar[last_b], (uses[last_b] - 1) & 1, err);
+        if (__syncthreads_or(lost)) {
+            ok = false;
+            break;
+        }
+        dhalo_load<CIN>(g, act, x0, y0, z0, Hs);
+        for (int i = t; i < (COUT / 8) * 128; i += kThreads) {
+            const int k = i % 128, q = i / 128;
+            const int64_t cell = ((int64_t)z0 * g.ny + y0 + k / 8) * g.nx + x0 + k % 8;
+            const uint4* src = reinterpret_cast<const uint4*>(grad + cell * COUT) + q;
+            asm volatile("cp.async.cg.shared.global [%0], [%1], 16;\n" ::"r"(tc::smem_addr(Bs + q * 2048 + k * 16)),
+                         "l"(src));
+        }
+        asm volatile("cp.async.wait_all;\n" ::: "memory");
+        __syncthreads();
+        for (int gi = 0; gi < G; ++gi, ++kg_run) {
+            const int b = kg_run & 1;
+            lost = uses[b] > 0 && !tc::mbar_wait(&bar[b], (uses[b] - 1) & 1, err);
+            if (__syncthreads_or(lost)) {
+                ok = false;
+                break;
+            }
+            unsigned char* A = As + b * WH::AB;
+            for (int i = t; i < TPG * QU * 128; i += kThreads) {
+                const int k = i % 128, kg = (i / 128) % QU, j = i / (128 * QU);
+                const int tap = gi * TPG + j;
+                uint4 v = make_uint4(0, 0, 0, 0);
+                if (tap < 27) {
+                    const int dx = tap % 3 - 1, dy = (tap / 3) % 3 - 1, dz = tap / 9 - 1;
+                    const int hu = ((kg * kHZ + 1 + dz) * kHY + 1 + dy + k / 8) * kHX + 1 + dx + k % 8;
+                    v = *reinterpret_cast<const uint4*>(Hs + hu * 16);
+                }
+                *reinterpret_cast<uint4*>(A + (j * QU + kg) * 2048 + k * 16) = v;
+            }
+            tc::fence_smem_async();
+            tc::fence_before_sync();
+            __syncthreads();
+            tc::fence_after_sync();
+            if (t == 0) {
+                const uint64_t da0 = tc::smem_desc(a0 + b * WH::AB, 128, 2048);
+                const uint64_t db0 = tc::smem_desc(b0, 128, 2048);
+#pragma unroll
+                for (int ks = 0; ks < 8; ++ks)
+                    tc::mma_bf16(tmem + gi * COUT, da0 + (uint32_t)(ks * 256 / 16), db0 + (uint32_t)(ks * 256 / 16),
+                                 idesc, (any || ks > 0) ? 1u : 0u);
+                tc::mma_commit(&bar[b]);
+            }
+            ++uses[b];
+            last_b = b;
+        }
+        any = true;
+    }
+    if (ok && last_b >= 0) {
+        const bool lost = !tc::mbar_wait(&bar[last_b], (uses[last_b] - 1) & 1, err);
+        ok = !__syncthreads_or(lost);
+    }
+    tc::fence_after_sync();
+    if (ok) {
+        const int w = t >> 5;
+        const int j = t / CIN, ci = t % CIN;
+        float* dst = partials + (int64_t)blockIdx.x * 27 * CIN * COUT;
+        for (int gi = 0; gi < G; ++gi) {
+            float v[COUT];
+            if (!any) {
+#pragma unroll
+                for (int co = 0; co < COUT; ++co) v[co] = 0.0f;
+            } else {
+#pragma unroll
+                for (int c0 = 0; c0 < COUT; c0 += 16)
+                    tc::tmem_ld16(tmem + ((uint32_t)(32 * w) << 16) + (uint32_t)(gi * COUT + c0), v + c0);
+            }
+            const int tap = gi * TPG + j;
+            if (tap < 27) {
+#pragma unroll
+                for (int co = 0; co < COUT; ++co) dst[((int64_t)tap * CIN + ci) * COUT + co] = v[co];
+            }
+        }
+    }
+    if (t == 0) {
+        for (int s = 0; s < 2; ++s)
+            if (uses[s] > 0) tc::mbar_wait(&bar[s], (uses[s] - 1) & 1, err);
+    }
+    tc::fence_before_sync();
+    __syncthreads();
+    if (t < 32) tc::tmem_dealloc(tmem, WH::TCOLS);
 }
 
 // out[j] = sum over p < P (in order) of partials[p * n + j].

@@ -116,25 +116,46 @@ template <int CIN, int COUT, int MODE>
 int run_conv(lbman_closure* c, cudaStream_t st, const __nv_bfloat16* in, const __nv_bfloat16* img,
              const float* bias, const __nv_bfloat16* pre_below, __nv_bfloat16* out_pre, __nv_bfloat16* out_bf,
              float* out_f) {
-    constexpr size_t smem = cl::bimg_bytes(CIN, COUT) + 2 * (CIN / 16) * 4096;
+    if (cl::dhalo_ok(c->nx, c->ny)) {
+        constexpr size_t smem = cl::bimg_bytes(CIN, COUT) + 2 * cl::dhalo_bytes(CIN);
+        constexpr auto K = cl::conv_dhalo_kernel<CIN, COUT, MODE>;
+        CL_CUDA(cudaFuncSetAttribute(K, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+        const int64_t tiles = (int64_t)(c->nx / 8) * (c->ny / 16) * c->nz;
+        const int grid = (int)std::min<int64_t>(tiles, (int64_t)resident<K>(cl::kThreads, smem) * c->num_sms);
+        const cl::Grid3 gr{c->nx, c->ny, c->nz, c->V};
+        K<<<grid, cl::kThreads, smem, st>>>(gr, in, reinterpret_cast<const uint4*>(img), bias, pre_below, out_pre,
+                                            out_bf, out_f, c->err);
+        CL_CUDA(cudaGetLastError());
+        return LBMAN_OK;
+    }
+    const int halo = cl::halo_ok(c->nx, c->ny) && cl::halo_bytes(c->nx, CIN) <= 96 * 1024 ? 1 : 0;
+    const size_t smem =
+        cl::bimg_bytes(CIN, COUT) + cl::kStages * (CIN / 16) * 4096 + (halo ? cl::halo_bytes(c->nx, CIN) : 0);
     constexpr auto K = cl::conv_kernel<CIN, COUT, MODE>;
     CL_CUDA(cudaFuncSetAttribute(K, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
     const int64_t tiles = (c->V + cl::kTileM - 1) / cl::kTileM;
     const int grid = (int)std::min<int64_t>(tiles, (int64_t)resident<K>(cl::kThreads, smem) * c->num_sms);
     const cl::Grid3 gr{c->nx, c->ny, c->nz, c->V};
     K<<<grid, cl::kThreads, smem, st>>>(gr, in, reinterpret_cast<const uint4*>(img), bias, pre_below, out_pre, out_bf,
-                                        out_f, c->err);
+                                        out_f, halo, c->err);
     CL_CUDA(cudaGetLastError());
     return LBMAN_OK;
 }
 
 template <int CIN, int COUT>
 int run_wgrad(lbman_closure* c, cudaStream_t st, const __nv_bfloat16* a, const __nv_bfloat16* gr, int layer) {
-    using WS = cl::WGradShape<CIN, COUT>;
-    constexpr auto K = cl::wgrad_kernel<CIN, COUT>;
-    CL_CUDA(cudaFuncSetAttribute(K, cudaFuncAttributeMaxDynamicSharedMemorySize, WS::SMEM));
     const cl::Grid3 g3{c->nx, c->ny, c->nz, c->V};
-    K<<<c->Gw, cl::kThreads, WS::SMEM, st>>>(g3, a, gr, c->wpart, c->err);
+    if (cl::dhalo_ok(c->nx, c->ny)) {
+        using WH = cl::WGradHalo<CIN, COUT>;
+        constexpr auto K = cl::wgrad_dhalo_kernel<CIN, COUT>;
+        CL_CUDA(cudaFuncSetAttribute(K, cudaFuncAttributeMaxDynamicSharedMemorySize, WH::SMEM));
+        K<<<c->Gw, cl::kThreads, WH::SMEM, st>>>(g3, a, gr, c->wpart, c->err);
+    } else {
+        using WS = cl::WGradShape<CIN, COUT>;
+        constexpr auto K = cl::wgrad_kernel<CIN, COUT>;
+        CL_CUDA(cudaFuncSetAttribute(K, cudaFuncAttributeMaxDynamicSharedMemorySize, WS::SMEM));
+        K<<<c->Gw, cl::kThreads, WS::SMEM, st>>>(g3, a, gr, c->wpart, c->err);
+    }
     CL_CUDA(cudaGetLastError());
     const int n = 27 * CIN * COUT;
     cl::sum_partials_kernel<<<(n + 255) / 256, 256, 0, st>>>(c->wpart, c->Gw, n, c->g + w_off(layer));
@@ -260,7 +281,7 @@ int lbman_closure_create(int device, int nx, int ny, int nz, uint64_t seed, lbma
     c->V = (int64_t)nx * ny * nz;
     cudaDeviceProp prop;
     if (cudaGetDeviceProperties(&prop, device) == cudaSuccess) c->num_sms = prop.multiProcessorCount;
-    c->Gw = c->num_sms;
+    c->Gw = 2 * c->num_sms;  // weight-gradient CTAs (two fit per SM in the staged form)
     c->Gb = 2 * c->num_sms;
     for (int j = 0; j < 9; ++j) {
         c->h_shift[j] = j == 0 ? 1.0f : 0.0f;

@@ -29,7 +29,9 @@ def test_tensor_core_selftest():
     assert np.all(e >= 0) and np.all(e < 1e-6), e
 
 
-@pytest.mark.parametrize("grid", [(8, 8, 8), (5, 6, 7), (16, 8, 4)])
+# (8, 8, 8), (5, 6, 7): gathers from global memory; (16, 16, 8), (64, 4, 4):
+# 128-cell tiles of whole x rows, staged through shared memory
+@pytest.mark.parametrize("grid", [(8, 8, 8), (5, 6, 7), (16, 16, 8), (64, 4, 4)])
 def test_forward_matches_oracle(grid):
     feat, _ = _case(grid, 1)
     with CL.Closure(*grid, seed=5) as cl:
@@ -41,7 +43,7 @@ def test_forward_matches_oracle(grid):
     assert np.max(np.abs(got - ref)) <= 2e-2 * np.max(np.abs(ref))
 
 
-@pytest.mark.parametrize("grid", [(8, 8, 8), (5, 6, 7)])
+@pytest.mark.parametrize("grid", [(8, 8, 8), (5, 6, 7), (16, 16, 8)])
 def test_gradient_matches_oracle(grid):
     feat, tgt = _case(grid, 2)
     with CL.Closure(*grid, seed=6) as cl:
