@@ -105,13 +105,15 @@ def run(fine_n=256, factor=4, zeta=0.01, train_seeds=(11, 12, 13), test_seed=99,
     fine.step(burn)
     cl.record(fine, new_trajectory=True)
     fine_stats, fine_fields = [], []
-    e0.record(stream)
+    fine_ms = 0.0
     for t in range(rollout):
+        e0.record(stream)
         fine.step(factor)
+        e1.record(stream)
+        e1.synchronize()
+        fine_ms += e0.elapsed_time(e1)
         cl.record(fine)
-    e1.record(stream)
-    e1.synchronize()
-    fine_ms = e0.elapsed_time(e1) / rollout
+    fine_ms /= rollout
     for t in range(rollout + 1):
         cl.load_snapshot(n0 + t, probe)
         if t >= rollout // 2:
