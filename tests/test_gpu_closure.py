@@ -82,3 +82,18 @@ def test_pipeline_trains_and_runs():
         cl.step(coarse, 3)
         out = coarse.download()
         assert np.all(np.isfinite(out["q"])) and np.all(np.isfinite(out["u"]))
+
+
+def test_trained_closure_beats_plain_coarse_on_held_out_run():
+    """What the network gains: after training on two seeds, one corrected
+    coarse step from a held-out filtered state is closer to the filtered
+    fine state than the plain coarse step, for Q and for u."""
+    from lbman3d_b200 import closure_experiment as X
+    r = X.run(fine_n=64, factor=4, zeta=0.01, train_seeds=(21, 22), test_seed=77, burn=200, snaps=20,
+              iters=300, lr=1e-3, rollout=6, log=lambda m: None)
+    first = r["short_time_relative_l2"][0]
+    assert first["step"] == 1
+    assert first["closure_q"] < first["plain_q"], first
+    assert first["closure_u"] < first["plain_u"], first
+    assert r["train"]["loss_last_tenth"] < r["train"]["loss_first_tenth"]
+    assert r["cost"]["closure_ms_per_coarse_step"] > 0
