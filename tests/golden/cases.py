@@ -32,6 +32,8 @@ BC = {
                   anch(0.3, 0.2, 0.5, 1), (1, Z3, 2, (0.0, 0.02, 0.0))],
     "qmixed": [PER, (1, Z3, 0, Z3), anch(0.5, 0.3, 0.2, 0), anch(0.5, 0.3, 0.2, 0), NEU_SPEC, NEU_NOSLIP],
     "walls": [NEU_NOSLIP] * 6,
+    # periodic Q with no-slip velocity walls on x (oracle-only larger-box case)
+    "qper_uwall": [(0, Z3, 1, Z3)] * 2 + [PER] * 4,
 }
 
 # Compile-time parameter sets of oracle/build_ref.py (physics only).

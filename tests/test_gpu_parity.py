@@ -71,6 +71,9 @@ BIG = [
     ("slit", (16, 33, 18), True),
     ("box_mixed", (13, 17, 19), False),
     ("lid", (31, 9, 14), True),
+    ("qmixed", (15, 14, 13), True),
+    ("qper_uwall", (18, 12, 10), False),
+    ("walls", (34, 10, 9), False),
 ]
 
 
