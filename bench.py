@@ -400,10 +400,13 @@ def main():
                     continue
                 s2, _ = make_sim(a.workload, prec, local)
                 s2.set_stream(stream.cuda_stream)
+                s2.init_seeded(1234, 0.5, 1e-3)
+                tuned2 = s2.autotune(steps_per_trial=3)
                 n2 = max(200, a.steps // 5)
                 ms2, _ = time_device(s2, n2, 10, stream)
                 variants[prec] = {"value": V * n2 / (ms2 * 1e3), "unit": "MLUPS", "steps": n2,
-                                  "frac": BYTES_PER_CELL[prec] * V / (ms2 / n2 * 1e-3) / 1e9 / peak}
+                                  "frac": BYTES_PER_CELL[prec] * V / (ms2 / n2 * 1e-3) / 1e9 / peak,
+                                  "shape": {k: tuned2[k] for k in ("kernels", "tile_x", "tile_y", "zchunk")}}
                 s2.close()
             line["variants"] = variants
             line["ensemble"] = ensemble_vs_sequential(local, stream)
