@@ -325,6 +325,32 @@ int lbman_closure_load_snapshot(lbman_closure* c, int k, lbman_solver* coarse);
  * rebuilt as f_eq, one solver step, then Q and u corrected.               */
 int lbman_closure_step(lbman_closure* c, lbman_solver* coarse, int nsteps);
 
+/* Disclination lines (the reference's DefectFinder::FindDefects,
+ * src/analysis/defect_finder.tpp): plaquette defect flags of the current Q on
+ * the device, then on the host the face connectivity graph and its
+ * decomposition into paths, as the reference builds them (same sweep order,
+ * same unordered-map / ordered-set graph, same greedy walk), so the lines and
+ * their count equal the reference's.  points (may be NULL) receives the face
+ * centres of every path, xyz, while 3 * (points so far) <= points_cap;
+ * line_offsets (may be NULL) receives the start of each path in points
+ * (line_offsets[0] = 0, then one entry per path, while the index < cap).
+ * Call once with NULL buffers to size them.  Every side needs >= 2 cells.  */
+typedef struct lbman_defects {
+    int64_t faces;            /* flagged plaquettes                           */
+    int64_t edges;            /* graph edges                                  */
+    int64_t lines;            /* paths (the reference's disclinations)        */
+    int64_t points;           /* path vertices over all lines                 */
+} lbman_defects;
+int lbman_defect_lines(lbman_solver* s, lbman_defects* info, double* points, int64_t points_cap,
+                       int64_t* line_offsets, int64_t offsets_cap);
+/* The same graph and paths from host flag arrays (def_x nx*(ny-1)*(nz-1),
+ * def_y (nx-1)*ny*(nz-1), def_z (nx-1)*(ny-1)*nz, x fastest, 1 = flagged);
+ * qper6[f] != 0 when face f's Q tag is periodic (QXoff wraps there).  Host
+ * only.                                                                     */
+int lbman_defect_graph(int nx, int ny, int nz, const int* qper6, const uint8_t* def_x, const uint8_t* def_y,
+                       const uint8_t* def_z, lbman_defects* info, double* points, int64_t points_cap,
+                       int64_t* line_offsets, int64_t offsets_cap);
+
 /* Steps completed since the last upload. */
 int lbman_steps_done(lbman_solver* s, int64_t* steps);
 /* Kernel launches issued by this solver since creation (instrumentation).  */

@@ -47,6 +47,10 @@ class lbman_shape(C.Structure):
                 ("threads", C.c_int), ("ms_per_step", C.c_double), ("blocks", C.c_int)]
 
 
+class lbman_defects(C.Structure):
+    _fields_ = [("faces", C.c_int64), ("edges", C.c_int64), ("lines", C.c_int64), ("points", C.c_int64)]
+
+
 class lbman_stats(C.Structure):
     _fields_ = [("mean_speed", C.c_double), ("rms_speed", C.c_double), ("defect_faces", C.c_int64),
                 ("defect_density", C.c_double)]
@@ -110,6 +114,11 @@ PROTOTYPES = [
     ("lbman_velocity_spectrum", C.c_int, [C.c_void_p, C.c_int, _DP, _DP]),
     ("lbman_q_correlation", C.c_int, [C.c_void_p, C.c_int, _DP, _DP, _DP]),
     ("lbman_statistics", C.c_int, [C.c_void_p, C.POINTER(lbman_stats)]),
+    ("lbman_defect_lines", C.c_int, [C.c_void_p, C.POINTER(lbman_defects), _DP, C.c_int64,
+                                     C.POINTER(C.c_int64), C.c_int64]),
+    ("lbman_defect_graph", C.c_int, [C.c_int, C.c_int, C.c_int, C.POINTER(C.c_int), C.c_void_p, C.c_void_p,
+                                     C.c_void_p, C.POINTER(lbman_defects), _DP, C.c_int64,
+                                     C.POINTER(C.c_int64), C.c_int64]),
     ("lbman_closure_selftest", C.c_int, [C.c_int, _DP]),
     ("lbman_closure_create", C.c_int, [C.c_int, C.c_int, C.c_int, C.c_int, C.c_uint64, C.POINTER(C.c_void_p)]),
     ("lbman_closure_destroy", C.c_int, [C.c_void_p]),
@@ -154,6 +163,24 @@ def check(status: int):
             raise DivergedError(status, msg)
         raise LbmanError(status, msg)
     return status
+
+
+def defect_graph(nx, ny, nz, qper6, def_x, def_y, def_z, with_points=True):
+    """lbman_defect_graph on host flag arrays: (info dict, points (n,3), offsets)."""
+    import numpy as np
+    fx, fy, fz = (np.ascontiguousarray(a, dtype=np.uint8) for a in (def_x, def_y, def_z))
+    q = (C.c_int * 6)(*[int(bool(v)) for v in qper6])
+    info = lbman_defects()
+    args = (int(nx), int(ny), int(nz), q, fx.ctypes.data_as(C.c_void_p), fy.ctypes.data_as(C.c_void_p),
+            fz.ctypes.data_as(C.c_void_p), C.byref(info))
+    check(lib().lbman_defect_graph(*args, None, 0, None, 0))
+    if not with_points:
+        return {k: getattr(info, k) for k, _ in lbman_defects._fields_}, None, None
+    pts = np.zeros(3 * max(info.points, 1))
+    off = np.zeros(info.lines + 1, dtype=np.int64)
+    check(lib().lbman_defect_graph(*args, pts.ctypes.data_as(_DP), pts.size,
+                                   off.ctypes.data_as(C.POINTER(C.c_int64)), off.size))
+    return {k: getattr(info, k) for k, _ in lbman_defects._fields_}, pts[:3 * info.points].reshape(-1, 3), off
 
 
 def fptr(a):

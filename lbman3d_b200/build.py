@@ -43,6 +43,7 @@ UNITS = {
     "noalloc.cu": [],
     "stats.cu": [],
     "closure_api.cu": [],
+    "defects.cu": [],
 }
 
 

@@ -8,6 +8,7 @@
 #include <cstdio>
 #include <cstring>
 #include <string>
+#include <vector>
 
 #include "../../include/lbman3d.h"
 #include "launch.h"
@@ -59,6 +60,7 @@ struct Ops {
     decltype(&launch_energy_reduce_f64) energy_reduce;
     decltype(&launch_director_f64) director;
     decltype(&launch_defect_count_f64) defect_count;
+    decltype(&launch_defect_flags_f64) defect_flags;
     decltype(&launch_seeded_init_f64) seeded_init;
     decltype(&qforce_smem_f64) qforce_smem;
     decltype(&qforce_threads_f64) qforce_threads;
@@ -71,7 +73,8 @@ struct Ops {
         launch_qforce_##SUF, launch_fused_##SUF, launch_lbm_##SUF, launch_stream_only_##SUF,           \
             launch_feq_init_##SUF, launch_pop_in_##SUF, launch_pop_out_##SUF, launch_real_in_##SUF,    \
             launch_real_out_##SUF, launch_flow_reduce_##SUF, launch_energy_reduce_##SUF,               \
-            launch_director_##SUF, launch_defect_count_##SUF, launch_seeded_init_##SUF,               \
+            launch_director_##SUF, launch_defect_count_##SUF, launch_defect_flags_##SUF,              \
+            launch_seeded_init_##SUF,                                                                  \
             qforce_smem_##SUF, qforce_threads_##SUF, march_blocks_##SUF, prepare_##SUF                 \
     }
 
@@ -698,6 +701,32 @@ int lbman_statistics(lbman_solver* s, lbman_stats* out) {
     out->defect_faces = d.defect_faces;
     out->defect_density = d.defect_faces >= 0 ? (double)d.defect_faces / (double)s->P.V : -1.0;
     return LBMAN_OK;
+}
+
+int lbman_defect_lines(lbman_solver* s, lbman_defects* info, double* points, int64_t points_cap,
+                       int64_t* line_offsets, int64_t offsets_cap) {
+    if (!s || !info) return fail(LBMAN_ERR_ARG, "null argument");
+    if (!s->uploaded) return fail(LBMAN_ERR_STATE, "defect lines before upload");
+    const int nx = s->P.nx, ny = s->P.ny, nz = s->P.nz;
+    if (nx < 2 || ny < 2 || nz < 2) return fail(LBMAN_ERR_ARG, "defect lines need at least 2 cells per side");
+    LB_TRY(set_device(s));
+    const int64_t V = s->P.V;
+    const int64_t nf = (int64_t)nx * (ny - 1) * (nz - 1) + (int64_t)(nx - 1) * ny * (nz - 1) +
+                       (int64_t)(nx - 1) * (ny - 1) * nz;
+    if (!s->dirbuf) LB_CUDA(cudaMalloc(&s->dirbuf, 3 * V * s->rbytes));
+    uint8_t* dflags = nullptr;
+    LB_CUDA(cudaMalloc(&dflags, (size_t)nf));
+    std::vector<uint8_t> flags((size_t)nf);
+    int st = check_launch(s, s->ops().director(s->P, s->q[s->qcur], nullptr, s->dirbuf, s->red_G, s->stream), "director");
+    if (st == LBMAN_OK) st = check_launch(s, s->ops().defect_flags(s->P, s->dirbuf, dflags, s->red_G, s->stream), "defect_flags");
+    if (st == LBMAN_OK && (cudaMemcpyAsync(flags.data(), dflags, (size_t)nf, cudaMemcpyDeviceToHost, s->stream) != cudaSuccess ||
+                           cudaStreamSynchronize(s->stream) != cudaSuccess))
+        st = fail(LBMAN_ERR_CUDA, "defect flags copy failed");
+    cudaFree(dflags);
+    if (st != LBMAN_OK) return st;
+    const int64_t nfx = (int64_t)nx * (ny - 1) * (nz - 1), nfy = (int64_t)(nx - 1) * ny * (nz - 1);
+    return lbman_defect_graph(nx, ny, nz, s->P.qper, flags.data(), flags.data() + nfx, flags.data() + nfx + nfy, info,
+                              points, points_cap, line_offsets, offsets_cap);
 }
 
 int lbman_get_shape(lbman_solver* s, lbman_shape* out) {

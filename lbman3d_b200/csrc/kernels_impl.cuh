@@ -234,6 +234,12 @@ cudaError_t director(const SimParams& P, const void* q, void* order, void* dir, 
     return cudaGetLastError();
 }
 template <class R>
+cudaError_t defect_flags(const SimParams& P, const void* dir, uint8_t* flags, int G, cudaStream_t st) {
+    defect_flags_kernel<R><<<G, kRedThreads, 0, st>>>(P, (const R*)dir, flags);
+    return cudaGetLastError();
+}
+
+template <class R>
 cudaError_t defect_count(const SimParams& P, const void* dir, double* partials, int G, cudaStream_t st) {
     defect_count_kernel<R><<<G, kRedThreads, 0, st>>>(P, (const R*)dir, partials);
     return cudaGetLastError();
@@ -322,6 +328,10 @@ cudaError_t prepare(size_t max_smem) {
     cudaError_t launch_director_##SUF(const SimParams& P, const void* q, void* order, void* dir, int G, \
                                       cudaStream_t st) {                                               \
         return impl::director<R>(P, q, order, dir, G, st);                                              \
+    }                                                                                                   \
+    cudaError_t launch_defect_flags_##SUF(const SimParams& P, const void* dir, uint8_t* flags, int G,  \
+                                          cudaStream_t st) {                                           \
+        return impl::defect_flags<R>(P, dir, flags, G, st);                                             \
     }                                                                                                   \
     cudaError_t launch_defect_count_##SUF(const SimParams& P, const void* dir, double* partials, int G, \
                                           cudaStream_t st) {                                           \

@@ -44,6 +44,8 @@ struct LaunchShape {
                                            cudaStream_t st);                                           \
     cudaError_t launch_director_##SUF(const SimParams& P, const void* q, void* order, void* dir, int G, \
                                       cudaStream_t st);                                                \
+    cudaError_t launch_defect_flags_##SUF(const SimParams& P, const void* dir, uint8_t* flags, int G,  \
+                                          cudaStream_t st);                                            \
     cudaError_t launch_defect_count_##SUF(const SimParams& P, const void* dir, double* partials, int G, \
                                           cudaStream_t st);                                            \
     cudaError_t launch_seeded_init_##SUF(const SimParams& P, uint64_t seed, double S0, double sigma,    \

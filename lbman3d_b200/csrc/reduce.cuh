@@ -185,6 +185,32 @@ __global__ void __launch_bounds__(kRedThreads) defect_count_kernel(SimParams P, 
     block_reduce_store<1, 0>(v, partials);
 }
 
+// Plaquette flags of the three face families in the reference's DefectFields
+// layout (src/analysis/defect_fields.h:16-29): def_x nx*(ny-1)*(nz-1), then
+// def_y (nx-1)*ny*(nz-1), then def_z (nx-1)*(ny-1)*nz, each x fastest.
+template <class R>
+__global__ void __launch_bounds__(kRedThreads) defect_flags_kernel(SimParams P, const R* __restrict__ dir,
+                                                                   uint8_t* __restrict__ flags) {
+    const int64_t V = P.V;
+    const int nx = P.nx, ny = P.ny, nz = P.nz;
+    const int64_t nfx = (int64_t)nx * (ny - 1) * (nz - 1), nfy = (int64_t)(nx - 1) * ny * (nz - 1);
+    auto D = [&](int x, int y, int z) { return dir + 3 * ((int64_t)z * P.nxy + (int64_t)y * nx + x); };
+    for (int64_t c = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; c < V; c += (int64_t)gridDim.x * blockDim.x) {
+        const int z = (int)(c / P.nxy);
+        const int rr = (int)(c - (int64_t)z * P.nxy);
+        const int y = rr / nx, x = rr - y * nx;
+        if (y < ny - 1 && z < nz - 1)
+            flags[((int64_t)z * (ny - 1) + y) * nx + x] =
+                (uint8_t)plaquette_flip<R>(D(x, y, z), D(x, y + 1, z), D(x, y + 1, z + 1), D(x, y, z + 1));
+        if (x < nx - 1 && z < nz - 1)
+            flags[nfx + ((int64_t)z * ny + y) * (nx - 1) + x] =
+                (uint8_t)plaquette_flip<R>(D(x, y, z), D(x + 1, y, z), D(x + 1, y, z + 1), D(x, y, z + 1));
+        if (x < nx - 1 && y < ny - 1)
+            flags[nfx + nfy + ((int64_t)z * (ny - 1) + y) * (nx - 1) + x] =
+                (uint8_t)plaquette_flip<R>(D(x, y, z), D(x + 1, y, z), D(x + 1, y + 1, z), D(x, y + 1, z));
+    }
+}
+
 // Pass 2: fold G partials of NQ quantities (the last nmax by max) in order.
 static __global__ void __launch_bounds__(1024) fold_partials_kernel(const double* __restrict__ partials, int G,
                                                              int nq, int nmax, double* __restrict__ out) {

@@ -149,6 +149,20 @@ class Simulation:
         N.check(N.lib().lbman_q_correlation(self._h, nb, N.dptr(Cb), N.dptr(n), C.byref(xi)))
         return Cb, n, xi.value
 
+    def defect_lines(self, with_points: bool = True):
+        """Disclination lines of the current Q, as the reference's
+        DefectFinder: (info dict, points (n, 3) face centres, line offsets)."""
+        info = N.lbman_defects()
+        N.check(N.lib().lbman_defect_lines(self._h, C.byref(info), None, 0, None, 0))
+        d = {k: getattr(info, k) for k, _ in N.lbman_defects._fields_}
+        if not with_points:
+            return d, None, None
+        pts = np.zeros(3 * max(info.points, 1))
+        off = np.zeros(info.lines + 1, dtype=np.int64)
+        N.check(N.lib().lbman_defect_lines(self._h, C.byref(info), N.dptr(pts), pts.size,
+                                           off.ctypes.data_as(C.POINTER(C.c_int64)), off.size))
+        return d, pts[:3 * info.points].reshape(-1, 3), off
+
     def statistics(self) -> dict:
         """Mean and rms speed, defect plaquettes and their density per cell."""
         st = N.lbman_stats()
