@@ -319,6 +319,10 @@ int lbman_closure_build_targets(lbman_closure* c, lbman_solver* coarse, int fit_
 /* Adam (beta 0.9 / 0.999) on random training pairs; loss_first/last receive
  * the mean loss of the first and last tenth of the iterations.            */
 int lbman_closure_train(lbman_closure* c, int iters, float lr, uint64_t seed, double* loss_first, double* loss_last);
+/* train_noise: std of Gaussian noise added to the normalised network inputs
+ * during lbman_closure_train (0 = none, the default); gain: multiplier of the
+ * correction in lbman_closure_step (1 = default).                          */
+int lbman_closure_set_options(lbman_closure* c, float train_noise, float gain);
 /* Coarse solver state := snapshot k.                                        */
 int lbman_closure_load_snapshot(lbman_closure* c, int k, lbman_solver* coarse);
 /* nsteps corrected coarse steps: network on the current state, populations

@@ -135,6 +135,7 @@ PROTOTYPES = [
     ("lbman_closure_train", C.c_int, [C.c_void_p, C.c_int, C.c_float, C.c_uint64, _DP, _DP]),
     ("lbman_closure_load_snapshot", C.c_int, [C.c_void_p, C.c_int, C.c_void_p]),
     ("lbman_closure_step", C.c_int, [C.c_void_p, C.c_void_p, C.c_int]),
+    ("lbman_closure_set_options", C.c_int, [C.c_void_p, C.c_float, C.c_float]),
     ("lbman_flow_reduce_noalloc", C.c_int,
      [C.c_int64, C.c_int, C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p, C.POINTER(lbman_diag)]),
 ]

@@ -50,7 +50,10 @@ class Closure:
 
     def close(self):
         if getattr(self, "_h", None):
-            N.lib().lbman_closure_destroy(self._h)
+            try:
+                N.lib().lbman_closure_destroy(self._h)
+            except (AttributeError, TypeError):  # interpreter shutdown: module globals already cleared
+                pass
             self._h = None
 
     def __del__(self):
@@ -115,6 +118,10 @@ class Closure:
 
     def load_snapshot(self, k: int, coarse):
         N.check(N.lib().lbman_closure_load_snapshot(self._h, int(k), coarse.handle))
+
+    def set_options(self, train_noise: float = 0.0, gain: float = 1.0):
+        """Input noise (std, normalised units) in training; correction gain."""
+        N.check(N.lib().lbman_closure_set_options(self._h, float(train_noise), float(gain)))
 
     def step(self, coarse, n: int = 1):
         N.check(N.lib().lbman_closure_step(self._h, coarse.handle, int(n)))

@@ -18,7 +18,9 @@ come from the training seeds; the held-out seed is the judge:
 * cost: device time per simulated coarse step of the fine solver (factor
   steps) against the corrected coarse solver (network + step), CUDA events.
 
-Prints one JSON object.  Fallback rule: the closure is reported ``usable``
+Training adds Gaussian noise (``--train-noise``, normalised units) to the
+network inputs, which makes the corrected runs drift less.  Prints one JSON
+object.  Fallback rule: the closure is reported ``usable``
 only if every statistic is within ``--tolerance`` of the fine run; otherwise
 the fine solver is the answer.
 """
@@ -50,7 +52,7 @@ def _rel(a, b):
 
 
 def run(fine_n=256, factor=4, zeta=0.01, train_seeds=(11, 12, 13), test_seed=99, burn=2000, snaps=120,
-        iters=3000, lr=1e-3, rollout=100, tolerance=0.05, log=print):
+        iters=3000, lr=1e-3, rollout=100, tolerance=0.05, train_noise=0.05, log=print):
     import torch
 
     import lbman3d_b200 as L
@@ -66,7 +68,8 @@ def run(fine_n=256, factor=4, zeta=0.01, train_seeds=(11, 12, 13), test_seed=99,
     stream = torch.cuda.current_stream()
     res = {"fine_grid": [fine_n] * 3, "coarse_grid": [nc] * 3, "factor": factor, "zeta": zeta,
            "train_seeds": list(train_seeds), "test_seed": test_seed, "burn_in_steps": burn,
-           "snapshots_per_seed": snaps, "train_iters": iters, "lr": lr, "rollout_coarse_steps": rollout,
+           "snapshots_per_seed": snaps, "train_iters": iters, "lr": lr, "train_input_noise": train_noise,
+           "rollout_coarse_steps": rollout,
            "coarse_params": {"TAUF": cp.TAUF, "GAMMA": cp.GAMMA, "L": cp.L, "ALPHA": cp.ALPHA}}
 
     fine = L.Simulation(fp, bc, L.Precision.FP32)
@@ -76,6 +79,7 @@ def run(fine_n=256, factor=4, zeta=0.01, train_seeds=(11, 12, 13), test_seed=99,
     for s in (fine, coarse, plain, probe):
         s.set_stream(stream.cuda_stream)
     cl = CL.Closure(nc, nc, nc, seed=1)
+    cl.set_options(train_noise=train_noise)
 
     # --- training data ---------------------------------------------------------
     for sd in train_seeds:
@@ -196,10 +200,12 @@ def main(argv=None):
     ap.add_argument("--rollout", type=int, default=100)
     ap.add_argument("--seeds", type=int, default=3)
     ap.add_argument("--tolerance", type=float, default=0.05)
+    ap.add_argument("--train-noise", type=float, default=0.05,
+                    help="std of Gaussian noise on the normalised inputs while training")
     a = ap.parse_args(argv)
     import sys
     res = run(a.fine, a.factor, a.zeta, tuple(range(11, 11 + a.seeds)), 99, a.burn, a.snaps, a.iters, a.lr,
-              a.rollout, a.tolerance, log=lambda m: print(m, file=sys.stderr, flush=True))
+              a.rollout, a.tolerance, a.train_noise, log=lambda m: print(m, file=sys.stderr, flush=True))
     print(json.dumps(res))
 
 

@@ -771,11 +771,27 @@ __global__ void adam_kernel(float* __restrict__ p, const float* __restrict__ gra
     }
 }
 
+// Standard normal variate from a counter (splitmix64 of key and index,
+// Box-Muller), for training-input noise.
+__device__ __forceinline__ float hash_normal(uint64_t key, uint64_t i) {
+    auto mix = [](uint64_t z) {
+        z += 0x9e3779b97f4a7c15ull;
+        z = (z ^ (z >> 30)) * 0xbf58476d1ce4e5b9ull;
+        z = (z ^ (z >> 27)) * 0x94d049bb133111ebull;
+        return z ^ (z >> 31);
+    };
+    const uint64_t h = mix(key ^ mix(i));
+    const float u1 = ((float)(h >> 40) + 0.5f) * 0x1.0p-24f, u2 = (float)((h >> 16) & 0xFFFFFF) * 0x1.0p-24f;
+    return sqrtf(-2.0f * logf(u1)) * cospif(2.0f * u2);
+}
+
 // Network input from 9 FP32 channel blocks (rho, u, Q; [9][V]):
-// act0[c][j] = (x_j - shift_j) * inv_scale_j for j < 9, 0 for j in 9..15.
+// act0[c][j] = (x_j - shift_j) * inv_scale_j (+ noise_std N(0,1) when
+// training with input noise) for j < 9, 0 for j in 9..15.
 __global__ void features_kernel(const float* __restrict__ rho, const float* __restrict__ u3,
                                 const float* __restrict__ q5, int64_t V, const float* __restrict__ shift,
-                                const float* __restrict__ inv_scale, __nv_bfloat16* __restrict__ act0) {
+                                const float* __restrict__ inv_scale, __nv_bfloat16* __restrict__ act0,
+                                float noise_std, uint64_t noise_key) {
     for (int64_t c = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; c < V; c += (int64_t)gridDim.x * blockDim.x) {
         __align__(16) __nv_bfloat16 v[16];
         float x[9];
@@ -785,7 +801,14 @@ __global__ void features_kernel(const float* __restrict__ rho, const float* __re
 #pragma unroll
         for (int k = 0; k < 5; ++k) x[4 + k] = q5[k * V + c];
 #pragma unroll
-        for (int j = 0; j < 16; ++j) v[j] = __float2bfloat16(j < 9 ? (x[j] - shift[j]) * inv_scale[j] : 0.0f);
+        for (int j = 0; j < 16; ++j) {
+            float f = 0.0f;
+            if (j < 9) {
+                f = (x[j] - shift[j]) * inv_scale[j];
+                if (noise_std > 0.0f) f += noise_std * hash_normal(noise_key, (uint64_t)c * 16 + j);
+            }
+            v[j] = __float2bfloat16(f);
+        }
         reinterpret_cast<uint4*>(act0 + c * 16)[0] = reinterpret_cast<const uint4*>(v)[0];
         reinterpret_cast<uint4*>(act0 + c * 16)[1] = reinterpret_cast<const uint4*>(v)[1];
     }
@@ -826,15 +849,15 @@ __global__ void __launch_bounds__(kThreads) loss_kernel(const float* __restrict_
     }
 }
 
-// Correction of a coarse state after its step: Q_k += out[c][k] * s_k
-// (k < 5), u_d += out[c][5+d] * s_{5+d}.
+// Correction of a coarse state after its step: Q_k += gain out[c][k] s_k
+// (k < 5), u_d += gain out[c][5+d] s_{5+d}.
 __global__ void apply_kernel(const float* __restrict__ out, const float* __restrict__ out_scale, int64_t V,
-                             float* __restrict__ u3, float* __restrict__ q5) {
+                             float gain, float* __restrict__ u3, float* __restrict__ q5) {
     for (int64_t c = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; c < V; c += (int64_t)gridDim.x * blockDim.x) {
 #pragma unroll
-        for (int k = 0; k < 5; ++k) q5[k * V + c] += out[c * 16 + k] * out_scale[k];
+        for (int k = 0; k < 5; ++k) q5[k * V + c] += gain * out[c * 16 + k] * out_scale[k];
 #pragma unroll
-        for (int d = 0; d < 3; ++d) u3[d * V + c] += out[c * 16 + 5 + d] * out_scale[5 + d];
+        for (int d = 0; d < 3; ++d) u3[d * V + c] += gain * out[c * 16 + 5 + d] * out_scale[5 + d];
     }
 }
 

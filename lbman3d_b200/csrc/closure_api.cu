@@ -108,6 +108,8 @@ struct lbman_closure {
     std::vector<float*> targets;
     std::vector<int> pair_src;
     int cur_traj = -1;
+    float train_noise = 0.0f;  // std of N(0,1) noise on the normalised inputs in training
+    float gain = 1.0f;         // correction multiplier in lbman_closure_step
 };
 
 namespace {
@@ -196,8 +198,10 @@ int upload_scales(lbman_closure* c) {
     return LBMAN_OK;
 }
 
-int features(lbman_closure* c, cudaStream_t st, const float* rho, const float* u3, const float* q5) {
-    cl::features_kernel<<<c->Gb, 256, 0, st>>>(rho, u3, q5, c->V, c->scales, c->scales + 9, c->act0);
+int features(lbman_closure* c, cudaStream_t st, const float* rho, const float* u3, const float* q5,
+             float noise_std = 0.0f, uint64_t noise_key = 0) {
+    cl::features_kernel<<<c->Gb, 256, 0, st>>>(rho, u3, q5, c->V, c->scales, c->scales + 9, c->act0, noise_std,
+                                                noise_key);
     CL_CUDA(cudaGetLastError());
     return LBMAN_OK;
 }
@@ -610,7 +614,7 @@ int lbman_closure_train(lbman_closure* c, int iters, float lr, uint64_t seed, do
         st ^= st << 17;
         const int pi = (int)(st % (uint64_t)npairs);
         const float* x = c->snaps[c->pair_src[pi]];
-        CL_TRY(features(c, c->stream, x, x + V, x + 4 * V));
+        CL_TRY(features(c, c->stream, x, x + V, x + 4 * V, c->train_noise, st));
         CL_TRY(forward(c, c->stream));
         CL_TRY(loss_grad(c, c->stream, c->targets[pi]));
         fold_loss_kernel<<<1, 32, 0, c->stream>>>(c->lpart, c->Gb, 1.0 / (8.0 * (double)V), c->loss_hist + it);
@@ -637,6 +641,13 @@ int lbman_closure_train(lbman_closure* c, int iters, float lr, uint64_t seed, do
     return LBMAN_OK;
 }
 
+int lbman_closure_set_options(lbman_closure* c, float train_noise, float gain) {
+    if (!c || !(train_noise >= 0.0f) || !(gain >= 0.0f)) return failc(LBMAN_ERR_ARG, "closure: bad options");
+    c->train_noise = train_noise;
+    c->gain = gain;
+    return LBMAN_OK;
+}
+
 int lbman_closure_step(lbman_closure* c, lbman_solver* coarse, int nsteps) {
     if (!c || !coarse || nsteps < 0) return failc(LBMAN_ERR_ARG, "closure: bad arguments");
     SolverView v;
@@ -652,8 +663,8 @@ int lbman_closure_step(lbman_closure* c, lbman_solver* coarse, int nsteps) {
         CL_TRY(solver_reset_populations(coarse));
         CL_TRY(lbman_step(coarse, 1));
         CL_TRY(solver_view(coarse, &w));
-        cl::apply_kernel<<<c->Gb, 256, 0, w.stream>>>(c->out, c->scales + 18, c->V, static_cast<float*>(w.u),
-                                                      static_cast<float*>(w.q));
+        cl::apply_kernel<<<c->Gb, 256, 0, w.stream>>>(c->out, c->scales + 18, c->V, c->gain,
+                                                      static_cast<float*>(w.u), static_cast<float*>(w.q));
         CL_CUDA(cudaGetLastError());
     }
     CL_CUDA(cudaStreamSynchronize(v.stream));
