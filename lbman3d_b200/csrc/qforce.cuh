@@ -84,31 +84,63 @@ __device__ __forceinline__ void cp_async16(float* s, const float* g) {
 }
 __device__ __forceinline__ void cp_async_wait_all() { asm volatile("cp.async.wait_all;\n" ::: "memory"); }
 
+// Source addresses of the 16-byte chunks (FP32 vec staging) that this
+// thread copies for every plane -- tile + 2-cell halo, all 8 variables --
+// without the plane offset.  Set once per column segment, so each plane's
+// copies cost one address add apiece.  Chunk k of thread t is chunk
+// i = t + k NT of the plane; its shared-memory offset within the plane slot
+// is 4 i (row-major rows of UX = 4 CH values).
+template <class TL, class R>
+struct PlaneSrc {
+    using ST = Stage<TL, R>;
+    static constexpr int CH = ST::UX / 4;
+    static constexpr int N = 8 * TL::UY * CH;
+    static constexpr int NCH = ST::VEC ? (N + TL::NT - 1) / TL::NT : 1;
+    const R* src[NCH];
+};
+
+template <class TL, class R>
+__device__ __forceinline__ void plane_src_init(const SimParams& P, int x0, int y0, const R* __restrict__ qin,
+                                               const R* __restrict__ uin, PlaneSrc<TL, R>& ps) {
+    using PS = PlaneSrc<TL, R>;
+    if constexpr (Stage<TL, R>::VEC) {
+#pragma unroll
+        for (int k = 0; k < PS::NCH; ++k) {
+            const int i = threadIdx.x + k * TL::NT;
+            if (i >= PS::N) {
+                ps.src[k] = qin;
+                continue;
+            }
+            const int row = i / PS::CH, ch = i - row * PS::CH;
+            const int var = row / TL::UY, ly = row - var * TL::UY;
+            const int gy = wrap_coord(y0 - 2 + ly, P.ny);
+            const int gx = wrap_coord(x0 - Stage<TL, R>::XO + 4 * ch, P.nx);
+            ps.src[k] = (var < 5 ? qin + (int64_t)var * P.V : uin + (int64_t)(var - 5) * P.V) +
+                        (int64_t)gy * P.nx + gx;
+        }
+    }
+}
+
 // Issue the copies of plane zg (Q then u, tile + 2-cell halo, periodic wrap)
 // into its ring slot; complete at the next cp_async_wait_all().  vec: 16-byte
-// chunks (FP32, nx a multiple of 4, 16-byte aligned fields), so no chunk
-// straddles the periodic seam.
+// chunks from the precomputed sources (FP32, nx a multiple of 4, 16-byte
+// aligned fields), so no chunk straddles the periodic seam.
 template <class TL, class R>
 __device__ __forceinline__ void qf_load_plane(const SimParams& P, int x0, int y0, int z0, int zg,
                                               const R* __restrict__ qin, const R* __restrict__ uin, R* QU,
-                                              bool vec) {
+                                              bool vec, const PlaneSrc<TL, R>& ps) {
     using ST = Stage<TL, R>;
     const int zw = wrap_coord(zg, P.nz);
     R* dst = QU + ring4(zg, z0) * 8 * ST::NQU;
     const int64_t zoff = (int64_t)zw * P.nxy;
     if constexpr (ST::VEC) {
         if (vec) {
-            constexpr int CH = ST::UX / 4;
-            constexpr int N = 8 * TL::UY * CH;
-#pragma unroll 1
-            for (int i = threadIdx.x; i < N; i += TL::NT) {
-                const int row = i / CH, ch = i - row * CH;
-                const int var = row / TL::UY, ly = row - var * TL::UY;
-                const int gy = wrap_coord(y0 - 2 + ly, P.ny);
-                const int gx = wrap_coord(x0 - ST::XO + 4 * ch, P.nx);
-                const R* src = (var < 5 ? qin + (int64_t)var * P.V : uin + (int64_t)(var - 5) * P.V) + zoff +
-                               (int64_t)gy * P.nx + gx;
-                cp_async16(dst + var * ST::NQU + ly * ST::UX + 4 * ch, src);
+            using PS = PlaneSrc<TL, R>;
+            R* d = dst + 4 * threadIdx.x;
+#pragma unroll
+            for (int k = 0; k < PS::NCH; ++k) {
+                if ((k + 1) * TL::NT <= PS::N || threadIdx.x + k * TL::NT < PS::N)
+                    cp_async16(d + 4 * k * TL::NT, ps.src[k] + zoff);
             }
             return;
         }
@@ -376,19 +408,21 @@ __device__ __forceinline__ void qf_march(const SimParams& P, int x0, int y0, int
     const bool vec = ST::VEC && (P.nx & 3) == 0 &&
                      ((reinterpret_cast<uintptr_t>(qin) | reinterpret_cast<uintptr_t>(uin)) & 15) == 0;
     R er_cur[3], er_next[3], qn_cur[5], qn_next[5];
+    PlaneSrc<TL, R> ps;
+    if (vec) plane_src_init<TL, R>(P, x0, y0, qin, uin, ps);
 
-    for (int z = z0 - 2; z <= z0 + 1; ++z) qf_load_plane<TL>(P, x0, y0, z0, z, qin, uin, QU, vec);
+    for (int z = z0 - 2; z <= z0 + 1; ++z) qf_load_plane<TL>(P, x0, y0, z0, z, qin, uin, QU, vec, ps);
     cp_async_wait_all();
     __syncthreads();
     qf_compute_plane<TL, R, UPWIND>(P, K, G, qx, qy, vx, vy, z0, z0 - 1, QU, Bs, er_next, qn_next);
     qf_compute_plane<TL, R, UPWIND>(P, K, G, qx, qy, vx, vy, z0, z0, QU, Bs, er_cur, qn_cur);
     __syncthreads();  // the slot of z0-2 is free again
-    qf_load_plane<TL>(P, x0, y0, z0, z0 + 2, qin, uin, QU, vec);
+    qf_load_plane<TL>(P, x0, y0, z0, z0 + 2, qin, uin, QU, vec, ps);
     cp_async_wait_all();
     __syncthreads();
 #pragma unroll 1
     for (int zc = z0; zc < z1; ++zc) {
-        if (zc + 1 < z1) qf_load_plane<TL>(P, x0, y0, z0, zc + 3, qin, uin, QU, vec);
+        if (zc + 1 < z1) qf_load_plane<TL>(P, x0, y0, z0, zc + 3, qin, uin, QU, vec, ps);
         qf_compute_plane<TL, R, UPWIND>(P, K, G, qx, qy, vx, vy, z0, zc + 1, QU, Bs, er_next, qn_next);
         __syncthreads();
         qf_force_cell<TL, R>(P, K, G, qx, qy, x0, y0, z0, zc, QU, Bs, er_cur, qn_cur, out);
