@@ -128,9 +128,18 @@ __device__ __forceinline__ R adv_deriv(R ux, R uy, R uz, const QD<R>& d) {
 // PointwiseStepAndSetupBodyForce (src/model.h:102-342): Q_new, Sigma, tau and
 // the Ericksen force -H:grad Q at one cell.
 template <class R, bool UPWIND>
+__device__ __forceinline__ void pointwise_q_mat(const Phys<R>& K, const R Q[5], R ux, R uy, R uz,
+                                                const QD<R> d[5], const GradU<R>& g, R qn[5], R sig[5],
+                                                R tau[3], R eric[3]);
+
+template <class R, bool UPWIND>
 __device__ __forceinline__ void pointwise_q(const Phys<R>& K, const R Q[5], R ux, R uy, R uz,
                                             const QD<R> d[5], const GradU<R>& g, R qn[5], R sig[5],
                                             R tau[3], R eric[3]) {
+    if constexpr (sizeof(R) == 4) {
+        pointwise_q_mat<R, UPWIND>(K, Q, ux, uy, uz, d, g, qn, sig, tau, eric);
+        return;
+    }
     const R A = K.A, B = K.B, C = K.C, L = K.L, LAMBDA = K.LAMBDA, GAMMA = K.GAMMA, DT = K.DT;
     const R Qxx = Q[0], Qxy = Q[1], Qxz = Q[2], Qyy = Q[3], Qyz = Q[4];
 
@@ -220,6 +229,96 @@ __device__ __forceinline__ void pointwise_q(const Phys<R>& K, const R Q[5], R ux
     qn[2] = Qxz + DT * (adv_xz + cor_xz + LAMBDA * (k23 * Exz + aln2_xz + aln3_xz) + GAMMA * Hxz);
     qn[3] = Qyy + DT * (adv_yy + cor_yy + LAMBDA * (k23 * Eyy + aln2_yy + aln3_yy) + GAMMA * Hyy);
     qn[4] = Qyz + DT * (adv_yz + cor_yz + LAMBDA * (k23 * Eyz + aln2_yz + aln3_yz) + GAMMA * Hyz);
+}
+
+// The same right-hand side for the FP32 instantiations, with the products of
+// two symmetric traceless tensors formed once as full matrices: for
+// M = Q E, QE + EQ = M + M^T; for N = Q H, QH + HQ = N + N^T and
+// tau = QH - HQ = N - N^T (HQ = (QH)^T), and tr = sum of the diagonal.  That
+// takes about 40 fewer operations per point than the reference's term-by-term
+// expansion (which the FP64 path keeps for bitwise parity); the values agree
+// to rounding.
+template <class R, bool UPWIND>
+__device__ __forceinline__ void pointwise_q_mat(const Phys<R>& K, const R Q[5], R ux, R uy, R uz,
+                                                const QD<R> d[5], const GradU<R>& g, R qn[5], R sig[5],
+                                                R tau[3], R eric[3]) {
+    const R A = K.A, B = K.B, C = K.C, L = K.L, LAMBDA = K.LAMBDA, GAMMA = K.GAMMA, DT = K.DT;
+    const R a = Q[0], b = Q[1], c = Q[2], e = Q[3], h = Q[4];  // Qxx Qxy Qxz Qyy Qyz
+    const R zz = -(a + e);                                     // Qzz
+    const R k23 = R(2.0 / 3.0);
+
+    // rhs_k: advection + co-rotation + LAMBDA (alignment), per component.
+    R rhs[5];
+#pragma unroll
+    for (int k = 0; k < 5; ++k) rhs[k] = -adv_deriv<R, UPWIND>(ux, uy, uz, d[k]);
+    {
+        const R Exx = g.ux_x, Eyy = g.uy_y, Ezz = -(Exx + Eyy);
+        const R Exy = R(0.5) * (g.ux_y + g.uy_x);
+        const R Exz = R(0.5) * (g.ux_z + g.uz_x);
+        const R Eyz = R(0.5) * (g.uy_z + g.uz_y);
+        const R Wxy = R(0.5) * (g.ux_y - g.uy_x);
+        const R Wxz = R(0.5) * (g.ux_z - g.uz_x);
+        const R Wyz = R(0.5) * (g.uy_z - g.uz_y);
+        rhs[0] += R(2.0) * (b * Wxy + c * Wxz);
+        rhs[1] += -a * Wxy + c * Wyz + e * Wxy + h * Wxz;
+        rhs[2] += R(-2.0) * a * Wxz - b * Wyz - e * Wxz + h * Wxy;
+        rhs[3] += R(2.0) * (-b * Wxy + h * Wyz);
+        rhs[4] += -a * Wyz - b * Wxz - c * Wxy - R(2.0) * e * Wyz;
+        // M = Q E
+        const R Mxx = a * Exx + b * Exy + c * Exz, Myy = b * Exy + e * Eyy + h * Eyz;
+        const R Mzz = c * Exz + h * Eyz + zz * Ezz;
+        const R trQE = Mxx + Myy + Mzz;
+        const R m2 = R(-2.0) * trQE;  // aln3 = -2 tr(QE) Q
+        const R kt = k23 * trQE;
+        rhs[0] += LAMBDA * (k23 * Exx + (R(2.0) * Mxx - kt) + m2 * a);
+        rhs[3] += LAMBDA * (k23 * Eyy + (R(2.0) * Myy - kt) + m2 * e);
+        const R Mxy = a * Exy + b * Eyy + c * Eyz, Myx = b * Exx + e * Exy + h * Exz;
+        rhs[1] += LAMBDA * (k23 * Exy + (Mxy + Myx) + m2 * b);
+        const R Mxz = a * Exz + b * Eyz + c * Ezz, Mzx = c * Exx + h * Exy + zz * Exz;
+        rhs[2] += LAMBDA * (k23 * Exz + (Mxz + Mzx) + m2 * c);
+        const R Myz = b * Exz + e * Eyz + h * Ezz, Mzy = c * Exy + h * Eyy + zz * Eyz;
+        rhs[4] += LAMBDA * (k23 * Eyz + (Myz + Mzy) + m2 * h);
+    }
+
+    R H[5];
+    {
+        const R TrQ2 = R(2.0) * (a * a + e * e + a * e + b * b + c * c + h * h);
+        const R t3 = R(1.0 / 3.0) * TrQ2;
+        const R ld = A + C * TrQ2;
+        H[0] = L * d[0].lap - ld * a - B * (a * a + b * b + c * c - t3);
+        H[1] = L * d[1].lap - ld * b - B * (a * b + b * e + c * h);
+        H[2] = L * d[2].lap - ld * c - B * (b * h - c * e);
+        H[3] = L * d[3].lap - ld * e - B * (b * b + e * e + h * h - t3);
+        H[4] = L * d[4].lap - ld * h - B * (b * c - h * a);
+    }
+    const R Hxx = H[0], Hxy = H[1], Hxz = H[2], Hyy = H[3], Hyz = H[4], Hzz = -(Hxx + Hyy);
+
+    eric[0] = R(-2.0) * (Hxx * d[0].dx + Hxy * d[1].dx + Hxz * d[2].dx + Hyy * d[3].dx + Hyz * d[4].dx) -
+              Hxx * d[3].dx - Hyy * d[0].dx;
+    eric[1] = R(-2.0) * (Hxx * d[0].dy + Hxy * d[1].dy + Hxz * d[2].dy + Hyy * d[3].dy + Hyz * d[4].dy) -
+              Hxx * d[3].dy - Hyy * d[0].dy;
+    eric[2] = R(-2.0) * (Hxx * d[0].dz + Hxy * d[1].dz + Hxz * d[2].dz + Hyy * d[3].dz + Hyz * d[4].dz) -
+              Hxx * d[3].dz - Hyy * d[0].dz;
+
+#pragma unroll
+    for (int k = 0; k < 5; ++k) qn[k] = Q[k] + DT * (rhs[k] + GAMMA * H[k]);
+
+    // N = Q H; sig = -2/3 LAMBDA H - LAMBDA (QH + HQ - 2/3 tr(QH) I) + 2 LAMBDA tr(QH) Q
+    const R Nxx = a * Hxx + b * Hxy + c * Hxz, Nyy = b * Hxy + e * Hyy + h * Hyz;
+    const R Nzz = c * Hxz + h * Hyz + zz * Hzz;
+    const R lt = LAMBDA * (Nxx + Nyy + Nzz);
+    const R mk23L = -k23 * LAMBDA;
+    sig[0] = mk23L * Hxx - LAMBDA * (R(2.0) * Nxx) + lt * (k23 + R(2.0) * a);
+    sig[3] = mk23L * Hyy - LAMBDA * (R(2.0) * Nyy) + lt * (k23 + R(2.0) * e);
+    const R Nxy = a * Hxy + b * Hyy + c * Hyz, Nyx = b * Hxx + e * Hxy + h * Hxz;
+    tau[0] = Nxy - Nyx;
+    sig[1] = mk23L * Hxy - LAMBDA * (Nxy + Nyx) + R(2.0) * lt * b;
+    const R Nxz = a * Hxz + b * Hyz + c * Hzz, Nzx = c * Hxx + h * Hxy + zz * Hxz;
+    tau[1] = Nxz - Nzx;
+    sig[2] = mk23L * Hxz - LAMBDA * (Nxz + Nzx) + R(2.0) * lt * c;
+    const R Nyz = b * Hxz + e * Hyz + h * Hzz, Nzy = c * Hxy + h * Hyy + zz * Hyz;
+    tau[2] = Nyz - Nzy;
+    sig[4] = mk23L * Hyz - LAMBDA * (Nyz + Nzy) + R(2.0) * lt * h;
 }
 
 // PointwiseSetActiveStressAndComputeBodyForce + PassiveStressDivergence sums

@@ -161,6 +161,7 @@ __device__ __forceinline__ void qf_load_plane(const SimParams& P, int x0, int y0
 // Per-thread geometry, fixed for the whole z march.
 struct PointGeo {
     int lbx, lby;     // position in the result region
+    int p;            // its index in the result planes, lby * BX + lbx
     int ax, ay;       // wrapped global coordinates of the point
     bool hasB, isC;   // owns a result point / a tile cell
     bool wx, wy, wz;  // block-uniform: wall rules may apply on this axis
@@ -171,8 +172,28 @@ __device__ __forceinline__ PointGeo point_geo(const SimParams& P, int x0, int y0
     PointGeo g;
     const int t = threadIdx.x;
     g.hasB = t < TL::NB;
-    g.lbx = t % TL::BX;
-    g.lby = t / TL::BX;
+    if constexpr (TL::BX >= 32) {
+        // Whole warps take 32-point row segments, so the stencil reads of a
+        // warp fall on consecutive shared-memory words (no bank conflicts);
+        // the last warp(s) take the TAIL leftover columns of every row.
+        constexpr int WPR = TL::BX / 32, NW = WPR * TL::BY, TAIL = TL::BX - 32 * WPR;
+        const int w = t >> 5;
+        if (w < NW) {
+            g.lby = w / WPR;
+            g.lbx = (w - g.lby * WPR) * 32 + (t & 31);
+        } else if constexpr (TAIL > 0) {
+            const int k = t - 32 * NW;
+            g.lby = k / TAIL;
+            g.lbx = 32 * WPR + (k - g.lby * TAIL);
+        } else {
+            g.lby = TL::BY;
+            g.lbx = 0;
+        }
+    } else {
+        g.lbx = t % TL::BX;
+        g.lby = t / TL::BX;
+    }
+    g.p = g.lby * TL::BX + g.lbx;
     g.ax = wrap_coord(x0 - 1 + g.lbx, P.nx);
     g.ay = wrap_coord(y0 - 1 + g.lby, P.ny);
     g.isC = g.hasB && g.lbx >= 1 && g.lbx <= TL::TCX && g.lby >= 1 && g.lby <= TL::TCY &&
@@ -247,8 +268,8 @@ __device__ __forceinline__ void qf_compute_plane(const SimParams& P, const Phys<
         // Row stress Pi_ab = Sigma_ab + tau_ab - ALPHA Q_new_ab (tau_ba = -tau_ab),
         // grouped by the axis b it is differentiated along (f_a = d_b Pi_ab).
         const R a = -K.ALPHA;
-        R* Bxy = Bs + ((zb - z0) & 1) * 6 * NB + threadIdx.x;
-        R* Bz = Bs + 12 * NB + ring3(zb, z0) * 3 * NB + threadIdx.x;
+        R* Bxy = Bs + ((zb - z0) & 1) * 6 * NB + G.p;
+        R* Bz = Bs + 12 * NB + ring3(zb, z0) * 3 * NB + G.p;
         Bxy[0 * NB] = sg[0] + a * qn[0];
         Bxy[1 * NB] = (sg[1] - ta[0]) + a * qn[1];
         Bxy[2 * NB] = (sg[2] - ta[1]) + a * qn[2];
@@ -259,7 +280,7 @@ __device__ __forceinline__ void qf_compute_plane(const SimParams& P, const Phys<
         Bz[1 * NB] = (sg[4] + ta[2]) + a * qn[4];
         Bz[2 * NB] = -(sg[0] + sg[3]) - a * (qn[0] + qn[3]);
     } else {
-        R* Bd = Bs + ring3(zb, z0) * 13 * NB + threadIdx.x;
+        R* Bd = Bs + ring3(zb, z0) * 13 * NB + G.p;
 #pragma unroll
         for (int k = 0; k < 5; ++k) Bd[k * NB] = qn[k];
 #pragma unroll
@@ -293,7 +314,7 @@ __device__ __forceinline__ void qf_force_cell(const SimParams& P, const Phys<R>&
     if (!G.isC) return;
     using ST = Stage<TL, R>;
     constexpr int NB = TL::NB, BX = TL::BX;
-    const int t = threadIdx.x;
+    const int t = G.p;
     const int gx = x0 + G.lbx - 1, gy = y0 + G.lby - 1;
     AxisRule qz;
     if (G.wz) qz = q_rule(P, 2, zc, P.nz);
