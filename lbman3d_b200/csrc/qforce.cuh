@@ -164,27 +164,39 @@ struct PointGeo {
     int p;            // its index in the result planes, lby * BX + lbx
     int ax, ay;       // wrapped global coordinates of the point
     bool hasB, isC;   // owns a result point / a tile cell
-    bool wx, wy, wz;  // block-uniform: wall rules may apply on this axis
+    bool wx, wy, wz;  // wall rules may apply on this axis: wz block-uniform,
+                      // wx / wy warp-uniform (see narrow_walls)
 };
 
 template <class TL>
 __device__ __forceinline__ PointGeo point_geo(const SimParams& P, int x0, int y0, int z0, int z1) {
     PointGeo g;
     const int t = threadIdx.x;
+    const bool perx = P.qper[0] && P.qper[1] && P.uper[0] && P.uper[1];
+    const bool pery = P.qper[2] && P.qper[3] && P.uper[2] && P.uper[3];
+    const bool perz = P.qper[4] && P.qper[5] && P.uper[4] && P.uper[5];
+    g.wx = !perx && (x0 - 1 < 1 || x0 + TL::TCX > P.nx - 2);
+    g.wy = !pery && (y0 - 1 < 1 || y0 + TL::TCY > P.ny - 2);
+    g.wz = !perz && (z0 - 1 < 1 || z1 > P.nz - 2);
     g.hasB = t < TL::NB;
     if constexpr (TL::BX >= 32) {
         // Whole warps take 32-point row segments, so the stencil reads of a
         // warp fall on consecutive shared-memory words (no bank conflicts);
-        // the last warp(s) take the TAIL leftover columns of every row.
+        // the last warp(s) take the TAIL leftover columns of every row.  In a
+        // block on the x-low wall the segments start at column 2, so the two
+        // wall-side columns (the wall point and the halo point beyond it)
+        // fall in the tail warp, as the x-high wall's columns already do.
         constexpr int WPR = TL::BX / 32, NW = WPR * TL::BY, TAIL = TL::BX - 32 * WPR;
+        const int s = (TAIL >= 2 && g.wx && x0 == 0) ? 2 : 0;
         const int w = t >> 5;
         if (w < NW) {
             g.lby = w / WPR;
-            g.lbx = (w - g.lby * WPR) * 32 + (t & 31);
+            g.lbx = s + (w - g.lby * WPR) * 32 + (t & 31);
         } else if constexpr (TAIL > 0) {
             const int k = t - 32 * NW;
             g.lby = k / TAIL;
-            g.lbx = 32 * WPR + (k - g.lby * TAIL);
+            const int j = k - g.lby * TAIL;
+            g.lbx = j < s ? j : j + 32 * WPR;
         } else {
             g.lby = TL::BY;
             g.lbx = 0;
@@ -198,13 +210,20 @@ __device__ __forceinline__ PointGeo point_geo(const SimParams& P, int x0, int y0
     g.ay = wrap_coord(y0 - 1 + g.lby, P.ny);
     g.isC = g.hasB && g.lbx >= 1 && g.lbx <= TL::TCX && g.lby >= 1 && g.lby <= TL::TCY &&
             x0 + g.lbx - 1 < P.nx && y0 + g.lby - 1 < P.ny;
-    const bool perx = P.qper[0] && P.qper[1] && P.uper[0] && P.uper[1];
-    const bool pery = P.qper[2] && P.qper[3] && P.uper[2] && P.uper[3];
-    const bool perz = P.qper[4] && P.qper[5] && P.uper[4] && P.uper[5];
-    g.wx = !perx && (x0 - 1 < 1 || x0 + TL::TCX > P.nx - 2);
-    g.wy = !pery && (y0 - 1 < 1 || y0 + TL::TCY > P.ny - 2);
-    g.wz = !perz && (z0 - 1 < 1 || z1 > P.nz - 2);
     return g;
+}
+
+// Narrows the block-uniform wx / wy to the warps that hold a point with a
+// wall rule on that axis (any clamp, ghost or wall flag of its Q or velocity
+// rule), so the other warps of a wall block skip the rule code.
+__device__ __forceinline__ void narrow_walls(PointGeo& g, const AxisRule& qx, const AxisRule& qy,
+                                             const VRule& vx, const VRule& vy) {
+    const bool fx = g.wx && (qx.m_clamp || qx.p_clamp || qx.m_ghost || qx.p_ghost || vx.m_clamp || vx.p_clamp ||
+                             vx.m_wall || vx.p_wall);
+    const bool fy = g.wy && (qy.m_clamp || qy.p_clamp || qy.m_ghost || qy.p_ghost || vy.m_clamp || vy.p_clamp ||
+                             vy.m_wall || vy.p_wall);
+    g.wx = __any_sync(0xffffffffu, fx);
+    g.wy = __any_sync(0xffffffffu, fy);
 }
 
 // Beris-Edwards update of this thread's point in plane zb; results to the
@@ -423,9 +442,10 @@ __device__ __forceinline__ void qf_march(const SimParams& P, int x0, int y0, int
     R* QU = smem;
     R* Bs = smem + 4 * 8 * ST::NQU;
     const Phys<R>& K = phys_ref<R>(P);
-    const PointGeo G = point_geo<TL>(P, x0, y0, z0, z1);
+    PointGeo G = point_geo<TL>(P, x0, y0, z0, z1);
     const AxisRule qx = q_rule(P, 0, G.ax, P.nx), qy = q_rule(P, 1, G.ay, P.ny);
     const VRule vx = v_rule(P, 0, G.ax, P.nx), vy = v_rule(P, 1, G.ay, P.ny);
+    narrow_walls(G, qx, qy, vx, vy);
     const bool vec = ST::VEC && (P.nx & 3) == 0 &&
                      ((reinterpret_cast<uintptr_t>(qin) | reinterpret_cast<uintptr_t>(uin)) & 15) == 0;
     R er_cur[3], er_next[3], qn_cur[5], qn_next[5];
