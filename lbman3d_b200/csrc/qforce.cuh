@@ -465,7 +465,9 @@ __device__ __forceinline__ void qf_march(const SimParams& P, int x0, int y0, int
     for (int zc = z0; zc < z1; ++zc) {
         if (zc + 1 < z1) qf_load_plane<TL>(P, x0, y0, z0, zc + 3, qin, uin, QU, vec, ps);
         qf_compute_plane<TL, R, UPWIND>(P, K, G, qx, qy, vx, vy, z0, zc + 1, QU, Bs, er_next, qn_next);
-        __syncthreads();
+        // No barrier here: the force of plane zc reads its neighbours' results
+        // of plane zc (written before the last barrier, in a slot that plane
+        // zc + 1 does not use) and the z-ring only at its own point.
         qf_force_cell<TL, R>(P, K, G, qx, qy, x0, y0, z0, zc, QU, Bs, er_cur, qn_cur, out);
 #pragma unroll
         for (int k = 0; k < 3; ++k) er_cur[k] = er_next[k];
