@@ -155,8 +155,12 @@ cudaError_t lbm(const SimParams& P, bool first, bool wr, const void* fin, void* 
                 void* rho, void* uout, cudaStream_t st) {
     const FastDiv dnx = make_fastdiv((uint32_t)P.nx), dnxy = make_fastdiv((uint32_t)P.nxy);
     const unsigned nb = blocks_for(P.V, 256);
-    lbm_kernel<R, S, DEV><<<nb, 256, 0, st>>>(P, dnx, dnxy, first ? 1 : 0, (const S*)fin, (S*)fout,
-                                              (const R*)F, (R*)rho, (R*)uout, wr ? 1 : 0);
+    if (P.uper[0] && P.uper[2] && P.uper[4])
+        lbm_kernel<R, S, DEV, false><<<nb, 256, 0, st>>>(P, dnx, dnxy, first ? 1 : 0, (const S*)fin, (S*)fout,
+                                                         (const R*)F, (R*)rho, (R*)uout, wr ? 1 : 0);
+    else
+        lbm_kernel<R, S, DEV, true><<<nb, 256, 0, st>>>(P, dnx, dnxy, first ? 1 : 0, (const S*)fin, (S*)fout,
+                                                        (const R*)F, (R*)rho, (R*)uout, wr ? 1 : 0);
     return cudaGetLastError();
 }
 

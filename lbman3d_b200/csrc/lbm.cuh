@@ -72,8 +72,9 @@ __device__ __forceinline__ bool touches_moving(const SimParams& P, int x, int y,
 }
 
 // Gather the 15 pre-collision populations of cell c from the post-collision
-// buffer fin (see the rule above).
-template <class R, class S>
+// buffer fin (see the rule above).  WALLS = false: every velocity axis is
+// periodic (wrap only, no wall logic compiled in).
+template <class R, class S, bool WALLS = true>
 __device__ __forceinline__ void gather(const SimParams& P, const Phys<R>& K, const S* __restrict__ fin,
                                        int64_t c, CellPos q, R rho_prev, R f[15]) {
     const int64_t V = P.V;
@@ -94,21 +95,28 @@ __device__ __forceinline__ void gather(const SimParams& P, const Phys<R>& K, con
         // source = c - e_j: e = +1 looks at the -1 neighbour
         const int64_t off = (ex_(j) > 0 ? ox_m : ex_(j) < 0 ? ox_p : 0) +
                             (ey_(j) > 0 ? oy_m : ey_(j) < 0 ? oy_p : 0) + (ez_(j) > 0 ? oz_m : ez_(j) < 0 ? oz_p : 0);
-        const bool cx = wx && ((ex_(j) > 0 && lox) || (ex_(j) < 0 && hix));
-        const bool cy = wy && ((ey_(j) > 0 && loy) || (ey_(j) < 0 && hiy));
-        const bool cz = wz && ((ez_(j) > 0 && loz) || (ez_(j) < 0 && hiz));
-        if (!(cx || cy || cz)) {
+        if constexpr (!WALLS) {
             f[j] = Store<S>::ld(fin + j * V + c + off);
             continue;
         }
-        const int cross = (cx ? 1 : 0) | (cy ? 2 : 0) | (cz ? 4 : 0);
-        const int fxs = ex_(j) > 0 ? 0 : 1, fys = ey_(j) > 0 ? 2 : 3, fzs = ez_(j) > 0 ? 4 : 5;
+        const bool cx = wx && ((ex_(j) > 0 && lox) || (ex_(j) < 0 && hix));
+        const bool cy = wy && ((ey_(j) > 0 && loy) || (ey_(j) < 0 && hiy));
+        const bool cz = wz && ((ez_(j) > 0 && loz) || (ez_(j) < 0 && hiz));
+        // Source slot: the neighbour's j, or for a wall crossing this cell's
+        // bi.  Only the index differs between the lanes, so a warp holding a
+        // wall lane still issues one load per direction.
+        int64_t src = j * V + c + off;
         int bi = -1, bf = 0;
-        if (cross & 1) { const int i = P.face[fxs].ubc == U_SPECULAR ? spec_(0, j) : opp_(j); if (i >= bi) { bi = i; bf = fxs; } }
-        if (cross & 2) { const int i = P.face[fys].ubc == U_SPECULAR ? spec_(1, j) : opp_(j); if (i >= bi) { bi = i; bf = fys; } }
-        if (cross & 4) { const int i = P.face[fzs].ubc == U_SPECULAR ? spec_(2, j) : opp_(j); if (i >= bi) { bi = i; bf = fzs; } }
-        R v = Store<S>::ld(fin + (int64_t)bi * V + c);
-        if (P.face[bf].ubc == U_MOVING) {
+        if (cx || cy || cz) {
+            const int cross = (cx ? 1 : 0) | (cy ? 2 : 0) | (cz ? 4 : 0);
+            const int fxs = ex_(j) > 0 ? 0 : 1, fys = ey_(j) > 0 ? 2 : 3, fzs = ez_(j) > 0 ? 4 : 5;
+            if (cross & 1) { const int i = P.face[fxs].ubc == U_SPECULAR ? spec_(0, j) : opp_(j); if (i >= bi) { bi = i; bf = fxs; } }
+            if (cross & 2) { const int i = P.face[fys].ubc == U_SPECULAR ? spec_(1, j) : opp_(j); if (i >= bi) { bi = i; bf = fys; } }
+            if (cross & 4) { const int i = P.face[fzs].ubc == U_SPECULAR ? spec_(2, j) : opp_(j); if (i >= bi) { bi = i; bf = fzs; } }
+            src = (int64_t)bi * V + c;
+        }
+        R v = Store<S>::ld(fin + src);
+        if (P.moving_any && bi >= 0 && P.face[bf].ubc == U_MOVING) {
             const R dot = R(ex_(j)) * K.uw[bf][0] + R(ey_(j)) * K.uw[bf][1] + R(ez_(j)) * K.uw[bf][2];
             v = v + R(6.0) * rho_prev * w_<R>(j) * dot;
         }
@@ -163,19 +171,20 @@ __device__ __forceinline__ void collide(const Phys<R>& K, R f[15], R Fx, R Fy, R
 
 // Pre-collision populations of cell c: read in place on the first step after
 // an upload, gathered from the neighbours' f* otherwise.
-template <class R, class S>
+template <class R, class S, bool WALLS = true>
 __device__ __forceinline__ void load_pre(const SimParams& P, const Phys<R>& K, bool first,
                                          const S* __restrict__ fin, int64_t c, CellPos q, R rho_prev, R f[15]) {
     if (first) {
 #pragma unroll
         for (int j = 0; j < 15; ++j) f[j] = Store<S>::ld(fin + j * P.V + c);
     } else {
-        gather<R, S>(P, K, fin, c, q, rho_prev, f);
+        gather<R, S, WALLS>(P, K, fin, c, q, rho_prev, f);
     }
 }
 
 // One LBM step.  first: fin holds pre-collision populations (just uploaded).
-template <class R, class S, bool DEV>
+// WALLS = false for boxes whose velocity axes are all periodic.
+template <class R, class S, bool DEV, bool WALLS>
 __global__ void __launch_bounds__(256) lbm_kernel(const __grid_constant__ SimParams P, FastDiv dnx, FastDiv dnxy, int first,
                                                   const S* __restrict__ fin, S* __restrict__ fout,
                                                   const R* __restrict__ F, R* __restrict__ rho_buf,
@@ -189,9 +198,9 @@ __global__ void __launch_bounds__(256) lbm_kernel(const __grid_constant__ SimPar
     const uint32_t r = (uint32_t)(c - (int64_t)q.z * P.nxy);
     q.y = (int)fdiv(r, dnx);
     q.x = (int)(r - (uint32_t)q.y * (uint32_t)P.nx);
-    const bool mv = P.moving_any && touches_moving(P, q.x, q.y, q.z);
+    const bool mv = WALLS && P.moving_any && touches_moving(P, q.x, q.y, q.z);
     R f[15];
-    load_pre<R, S>(P, K, first != 0, fin, c, q, (mv && !first) ? rho_buf[c] : R(0), f);
+    load_pre<R, S, WALLS>(P, K, first != 0, fin, c, q, (mv && !first) ? rho_buf[c] : R(0), f);
     R rho, ux, uy, uz;
     collide<R, DEV>(K, f, F[c], F[V + c], F[2 * V + c], rho, ux, uy, uz);
 #pragma unroll
