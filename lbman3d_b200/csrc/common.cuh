@@ -113,16 +113,24 @@ __host__ __device__ constexpr R w_(int i) {
 
 // Storage conversions for populations.
 template <class S> struct Store;
+// ld = raw load + widen; the split form lets a gather issue every load before
+// the first conversion waits on one.
 template <> struct Store<double> {
     __device__ static double ld(const double* p) { return __ldg(p); }
+    __device__ static double raw(const double* p) { return __ldg(p); }
+    __device__ static double widen(double v) { return v; }
     __device__ static void st(double* p, double v) { *p = v; }
 };
 template <> struct Store<float> {
     __device__ static float ld(const float* p) { return __ldg(p); }
+    __device__ static float raw(const float* p) { return __ldg(p); }
+    __device__ static float widen(float v) { return v; }
     __device__ static void st(float* p, float v) { *p = v; }
 };
 template <> struct Store<__half> {
     __device__ static float ld(const __half* p) { return __half2float(__ldg(p)); }
+    __device__ static __half raw(const __half* p) { return __ldg(p); }
+    __device__ static float widen(__half v) { return __half2float(v); }
     __device__ static void st(__half* p, float v) { *p = __float2half_rn(v); }
 };
 

@@ -71,6 +71,21 @@ __device__ __forceinline__ bool touches_moving(const SimParams& P, int x, int y,
            (z == 0 && P.face[4].ubc == U_MOVING) || (z == P.nz - 1 && P.face[5].ubc == U_MOVING);
 }
 
+// The direction whose post-collision value at this cell the reference's
+// wall rules leave in slot j when c - e_j lies beyond the crossed walls
+// (cx, cy, cz): per crossed axis the candidate opp(j) (no-slip / moving) or
+// spec_A(j) (specular); the largest wins, ties to the later axis.  *face, if
+// given, receives the winning wall.
+__device__ __forceinline__ int wall_source(const SimParams& P, int j, bool cx, bool cy, bool cz, int* face) {
+    const int fxs = ex_(j) > 0 ? 0 : 1, fys = ey_(j) > 0 ? 2 : 3, fzs = ez_(j) > 0 ? 4 : 5;
+    int bi = -1, bf = 0;
+    if (cx) { const int i = P.face[fxs].ubc == U_SPECULAR ? spec_(0, j) : opp_(j); if (i >= bi) { bi = i; bf = fxs; } }
+    if (cy) { const int i = P.face[fys].ubc == U_SPECULAR ? spec_(1, j) : opp_(j); if (i >= bi) { bi = i; bf = fys; } }
+    if (cz) { const int i = P.face[fzs].ubc == U_SPECULAR ? spec_(2, j) : opp_(j); if (i >= bi) { bi = i; bf = fzs; } }
+    if (face) *face = bf;
+    return bi;
+}
+
 // Gather the 15 pre-collision populations of cell c from the post-collision
 // buffer fin (see the rule above).  WALLS = false: every velocity axis is
 // periodic (wrap only, no wall logic compiled in).
@@ -90,13 +105,16 @@ __device__ __forceinline__ void gather(const SimParams& P, const Phys<R>& K, con
     const int64_t oz_m = loz ? (int64_t)(nz - 1) * P.nxy : -P.nxy;
     const int64_t oz_p = hiz ? -(int64_t)(nz - 1) * P.nxy : P.nxy;
     const bool wx = !P.uper[0], wy = !P.uper[2], wz = !P.uper[4];
+    // Pass 1 issues the 15 loads (raw storage values), pass 2 widens them,
+    // pass 3 adds the moving-wall term; no load waits inside pass 1.
+    S raw[15];
 #pragma unroll
     for (int j = 0; j < 15; ++j) {
         // source = c - e_j: e = +1 looks at the -1 neighbour
         const int64_t off = (ex_(j) > 0 ? ox_m : ex_(j) < 0 ? ox_p : 0) +
                             (ey_(j) > 0 ? oy_m : ey_(j) < 0 ? oy_p : 0) + (ez_(j) > 0 ? oz_m : ez_(j) < 0 ? oz_p : 0);
         if constexpr (!WALLS) {
-            f[j] = Store<S>::ld(fin + j * V + c + off);
+            raw[j] = Store<S>::raw(fin + j * V + c + off);
             continue;
         }
         const bool cx = wx && ((ex_(j) > 0 && lox) || (ex_(j) < 0 && hix));
@@ -106,21 +124,27 @@ __device__ __forceinline__ void gather(const SimParams& P, const Phys<R>& K, con
         // bi.  Only the index differs between the lanes, so a warp holding a
         // wall lane still issues one load per direction.
         int64_t src = j * V + c + off;
-        int bi = -1, bf = 0;
-        if (cx || cy || cz) {
-            const int cross = (cx ? 1 : 0) | (cy ? 2 : 0) | (cz ? 4 : 0);
-            const int fxs = ex_(j) > 0 ? 0 : 1, fys = ey_(j) > 0 ? 2 : 3, fzs = ez_(j) > 0 ? 4 : 5;
-            if (cross & 1) { const int i = P.face[fxs].ubc == U_SPECULAR ? spec_(0, j) : opp_(j); if (i >= bi) { bi = i; bf = fxs; } }
-            if (cross & 2) { const int i = P.face[fys].ubc == U_SPECULAR ? spec_(1, j) : opp_(j); if (i >= bi) { bi = i; bf = fys; } }
-            if (cross & 4) { const int i = P.face[fzs].ubc == U_SPECULAR ? spec_(2, j) : opp_(j); if (i >= bi) { bi = i; bf = fzs; } }
-            src = (int64_t)bi * V + c;
+        if (cx || cy || cz) src = (int64_t)wall_source(P, j, cx, cy, cz, nullptr) * V + c;
+        raw[j] = Store<S>::raw(fin + src);
+    }
+#pragma unroll
+    for (int j = 0; j < 15; ++j) f[j] = Store<S>::widen(raw[j]);
+    if constexpr (WALLS) {
+        if (P.moving_any) {
+#pragma unroll
+            for (int j = 0; j < 15; ++j) {
+                const bool cx = wx && ((ex_(j) > 0 && lox) || (ex_(j) < 0 && hix));
+                const bool cy = wy && ((ey_(j) > 0 && loy) || (ey_(j) < 0 && hiy));
+                const bool cz = wz && ((ez_(j) > 0 && loz) || (ez_(j) < 0 && hiz));
+                if (!(cx || cy || cz)) continue;
+                int bf;
+                wall_source(P, j, cx, cy, cz, &bf);
+                if (P.face[bf].ubc == U_MOVING) {
+                    const R dot = R(ex_(j)) * K.uw[bf][0] + R(ey_(j)) * K.uw[bf][1] + R(ez_(j)) * K.uw[bf][2];
+                    f[j] = f[j] + R(6.0) * rho_prev * w_<R>(j) * dot;
+                }
+            }
         }
-        R v = Store<S>::ld(fin + src);
-        if (P.moving_any && bi >= 0 && P.face[bf].ubc == U_MOVING) {
-            const R dot = R(ex_(j)) * K.uw[bf][0] + R(ey_(j)) * K.uw[bf][1] + R(ez_(j)) * K.uw[bf][2];
-            v = v + R(6.0) * rho_prev * w_<R>(j) * dot;
-        }
-        f[j] = v;
     }
 }
 
@@ -182,10 +206,19 @@ __device__ __forceinline__ void load_pre(const SimParams& P, const Phys<R>& K, b
     }
 }
 
+// Resident blocks per SM the LBM kernel's registers are held to (measured
+// on B200: the walled form keeps its 15 loads in flight within 5 blocks per
+// SM, 2 for FP64; the periodic form's natural budgets are 5 / 6 / 3 blocks for
+// FP32 / FP16 storage / FP64).
+template <class R, class S, bool WALLS>
+constexpr int lbm_min_blocks() {
+    return sizeof(R) == 8 ? (WALLS ? 2 : 3) : (sizeof(S) == 2 && !WALLS ? 6 : 5);
+}
+
 // One LBM step.  first: fin holds pre-collision populations (just uploaded).
 // WALLS = false for boxes whose velocity axes are all periodic.
 template <class R, class S, bool DEV, bool WALLS>
-__global__ void __launch_bounds__(256) lbm_kernel(const __grid_constant__ SimParams P, FastDiv dnx, FastDiv dnxy, int first,
+__global__ void __launch_bounds__(256, lbm_min_blocks<R, S, WALLS>()) lbm_kernel(const __grid_constant__ SimParams P, FastDiv dnx, FastDiv dnxy, int first,
                                                   const S* __restrict__ fin, S* __restrict__ fout,
                                                   const R* __restrict__ F, R* __restrict__ rho_buf,
                                                   R* __restrict__ uout, int write_rho_all) {
