@@ -243,7 +243,25 @@ def error_vs_fp64(workload, precision, device, nsteps=100):
     return out
 
 
-def time_e2e(sim, p, iters, stream, save_interval=100):
+def reduce_max(value, world, device):
+    """The maximum of a per-rank float over all ranks (the value itself on one
+    rank).  Every rank must call it, in the same order."""
+    if world == 1:
+        return float(value)
+    import torch
+    import torch.distributed as dist
+    t = torch.tensor([float(value)], dtype=torch.float64, device=device)
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return float(t.item())
+
+
+def whole_job_rate(cells_per_rank, steps, world, ms_max):
+    """MLUPS of the whole job: every rank advanced its own box of
+    cells_per_rank cells by `steps` steps, the slowest rank in ms_max."""
+    return world * cells_per_rank * steps / (ms_max * 1e3)
+
+
+def time_e2e(sim, p, iters, stream, save_interval=100, world=1, device=None):
     import torch
     V = p.V
     pin = lambda n: torch.empty(n, dtype=torch.float64, pin_memory=True).numpy()
@@ -268,10 +286,10 @@ def time_e2e(sim, p, iters, stream, save_interval=100):
         cycle()
     e1.record(stream)
     e1.synchronize()
-    ms = e0.elapsed_time(e1)
-    mlups = V * save_interval * iters / (ms * 1e3)
-    return {"value": mlups, "unit": "MLUPS", "h2d_bytes_per_step": 9 * V * 8, "d2h_bytes_per_step": 9 * V * 8,
-            "solver_steps_per_step": save_interval, "steps": iters}
+    ms = reduce_max(e0.elapsed_time(e1), world, device)
+    mlups = whole_job_rate(V, save_interval * iters, world, ms)
+    return {"value": mlups, "unit": "MLUPS", "h2d_bytes_per_step": world * 9 * V * 8,
+            "d2h_bytes_per_step": world * 9 * V * 8, "solver_steps_per_step": save_interval, "steps": iters}
 
 
 def reference_cpu(workload, max_steps, warmup):
@@ -349,7 +367,8 @@ def main():
     import torch.distributed as dist
     local = int(os.environ.get("LOCAL_RANK", "0"))
     if world > 1:
-        dist.init_process_group("nccl", init_method="env://")
+        import datetime
+        dist.init_process_group("nccl", init_method="env://", timeout=datetime.timedelta(seconds=300))
     torch.cuda.set_device(local)
     stream = torch.cuda.Stream(device=local)
 
@@ -368,12 +387,9 @@ def main():
     torch.cuda.synchronize()
     with ClockSampler(local) as clk:
         ms, launches = time_device(sim, a.steps, max(a.warmup, 3), stream)
-    if world > 1:
-        t = torch.tensor([ms], device="cuda")
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        ms = float(t.item())
+    ms = reduce_max(ms, world, "cuda")
     ms_step = ms / a.steps
-    mlups = world * V * a.steps / (ms * 1e3)
+    mlups = whole_job_rate(V, a.steps, world, ms)
     peak, peak_kind = measured_peaks()
     bpc = BYTES_PER_CELL[a.precision]
     step_achieved = bpc * V / (ms_step * 1e-3) / 1e9
@@ -391,8 +407,8 @@ def main():
                          "step_frac": step_achieved / peak},
             "clocks": clk.summary()}
     if not a.no_extras:
-        line["e2e"] = time_e2e(sim, p, 5, stream)
-        if rank == 0:
+        line["e2e"] = time_e2e(sim, p, 5, stream, world=world, device="cuda")
+        if world == 1:  # single-GPU extras; at N > 1 every rank runs only the legs above
             line["error_vs_fp64"] = error_vs_fp64(a.workload, a.precision, local) if a.precision != "fp64" else None
             variants = {}
             for prec in ("fp64", "fp16"):
