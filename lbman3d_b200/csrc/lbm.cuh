@@ -89,21 +89,24 @@ __device__ __forceinline__ int wall_source(const SimParams& P, int j, bool cx, b
 // Gather the 15 pre-collision populations of cell c from the post-collision
 // buffer fin (see the rule above).  WALLS = false: every velocity axis is
 // periodic (wrap only, no wall logic compiled in).
-template <class R, class S, bool WALLS = true>
+// I: index type of the population offsets -- int when 15 V < 2^31 (the
+// launcher checks), so addresses take 32-bit arithmetic.
+template <class R, class S, bool WALLS = true, class I = int64_t>
 __device__ __forceinline__ void gather(const SimParams& P, const Phys<R>& K, const S* __restrict__ fin,
-                                       int64_t c, CellPos q, R rho_prev, R f[15]) {
-    const int64_t V = P.V;
+                                       I c, CellPos q, R rho_prev, R f[15]) {
+    const I V = (I)P.V;
     const int nx = P.nx, ny = P.ny, nz = P.nz;
     // Offsets of the source cell c - e along each axis for e = +1 / -1, with
     // the periodic wrap folded in, and whether that source lies beyond a wall
     // (velocity tags are periodic on both faces of an axis or on neither).
     const bool lox = q.x == 0, hix = q.x == nx - 1, loy = q.y == 0, hiy = q.y == ny - 1;
     const bool loz = q.z == 0, hiz = q.z == nz - 1;
-    const int64_t ox_m = lox ? (int64_t)(nx - 1) : -1, ox_p = hix ? (int64_t)(1 - nx) : 1;
-    const int64_t oy_m = loy ? (int64_t)(ny - 1) * nx : -(int64_t)nx;
-    const int64_t oy_p = hiy ? -(int64_t)(ny - 1) * nx : (int64_t)nx;
-    const int64_t oz_m = loz ? (int64_t)(nz - 1) * P.nxy : -P.nxy;
-    const int64_t oz_p = hiz ? -(int64_t)(nz - 1) * P.nxy : P.nxy;
+    const I nxy = (I)P.nxy;
+    const I ox_m = lox ? (I)(nx - 1) : (I)-1, ox_p = hix ? (I)(1 - nx) : (I)1;
+    const I oy_m = loy ? (I)(ny - 1) * nx : -(I)nx;
+    const I oy_p = hiy ? -(I)(ny - 1) * nx : (I)nx;
+    const I oz_m = loz ? (I)(nz - 1) * nxy : -nxy;
+    const I oz_p = hiz ? -(I)(nz - 1) * nxy : nxy;
     const bool wx = !P.uper[0], wy = !P.uper[2], wz = !P.uper[4];
     // Pass 1 issues the 15 loads (raw storage values), pass 2 widens them,
     // pass 3 adds the moving-wall term; no load waits inside pass 1.
@@ -111,10 +114,10 @@ __device__ __forceinline__ void gather(const SimParams& P, const Phys<R>& K, con
 #pragma unroll
     for (int j = 0; j < 15; ++j) {
         // source = c - e_j: e = +1 looks at the -1 neighbour
-        const int64_t off = (ex_(j) > 0 ? ox_m : ex_(j) < 0 ? ox_p : 0) +
-                            (ey_(j) > 0 ? oy_m : ey_(j) < 0 ? oy_p : 0) + (ez_(j) > 0 ? oz_m : ez_(j) < 0 ? oz_p : 0);
+        const I off = (ex_(j) > 0 ? ox_m : ex_(j) < 0 ? ox_p : (I)0) +
+                      (ey_(j) > 0 ? oy_m : ey_(j) < 0 ? oy_p : (I)0) + (ez_(j) > 0 ? oz_m : ez_(j) < 0 ? oz_p : (I)0);
         if constexpr (!WALLS) {
-            raw[j] = Store<S>::raw(fin + j * V + c + off);
+            raw[j] = Store<S>::raw(fin + (j * V + c + off));
             continue;
         }
         const bool cx = wx && ((ex_(j) > 0 && lox) || (ex_(j) < 0 && hix));
@@ -123,8 +126,8 @@ __device__ __forceinline__ void gather(const SimParams& P, const Phys<R>& K, con
         // Source slot: the neighbour's j, or for a wall crossing this cell's
         // bi.  Only the index differs between the lanes, so a warp holding a
         // wall lane still issues one load per direction.
-        int64_t src = j * V + c + off;
-        if (cx || cy || cz) src = (int64_t)wall_source(P, j, cx, cy, cz, nullptr) * V + c;
+        I src = j * V + c + off;
+        if (cx || cy || cz) src = (I)wall_source(P, j, cx, cy, cz, nullptr) * V + c;
         raw[j] = Store<S>::raw(fin + src);
     }
 #pragma unroll
@@ -195,14 +198,14 @@ __device__ __forceinline__ void collide(const Phys<R>& K, R f[15], R Fx, R Fy, R
 
 // Pre-collision populations of cell c: read in place on the first step after
 // an upload, gathered from the neighbours' f* otherwise.
-template <class R, class S, bool WALLS = true>
+template <class R, class S, bool WALLS = true, class I = int64_t>
 __device__ __forceinline__ void load_pre(const SimParams& P, const Phys<R>& K, bool first,
-                                         const S* __restrict__ fin, int64_t c, CellPos q, R rho_prev, R f[15]) {
+                                         const S* __restrict__ fin, I c, CellPos q, R rho_prev, R f[15]) {
     if (first) {
 #pragma unroll
-        for (int j = 0; j < 15; ++j) f[j] = Store<S>::ld(fin + j * P.V + c);
+        for (int j = 0; j < 15; ++j) f[j] = Store<S>::ld(fin + (j * (I)P.V + c));
     } else {
-        gather<R, S, WALLS>(P, K, fin, c, q, rho_prev, f);
+        gather<R, S, WALLS, I>(P, K, fin, c, q, rho_prev, f);
     }
 }
 
@@ -216,24 +219,25 @@ constexpr int lbm_min_blocks() {
 }
 
 // One LBM step.  first: fin holds pre-collision populations (just uploaded).
-// WALLS = false for boxes whose velocity axes are all periodic.
-template <class R, class S, bool DEV, bool WALLS>
+// WALLS = false for boxes whose velocity axes are all periodic; I = int when
+// 15 V < 2^31 (32-bit index arithmetic), else int64_t.
+template <class R, class S, bool DEV, bool WALLS, class I>
 __global__ void __launch_bounds__(256, lbm_min_blocks<R, S, WALLS>()) lbm_kernel(const __grid_constant__ SimParams P, FastDiv dnx, FastDiv dnxy, int first,
                                                   const S* __restrict__ fin, S* __restrict__ fout,
                                                   const R* __restrict__ F, R* __restrict__ rho_buf,
                                                   R* __restrict__ uout, int write_rho_all) {
-    const int64_t c = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
-    if (c >= P.V) return;
-    const int64_t V = P.V;
+    const I c = (I)blockIdx.x * (I)blockDim.x + (I)threadIdx.x;
+    if (c >= (I)P.V) return;
+    const I V = (I)P.V;
     const Phys<R>& K = phys_ref<R>(P);
     CellPos q;
     q.z = (int)fdiv((uint32_t)c, dnxy);
-    const uint32_t r = (uint32_t)(c - (int64_t)q.z * P.nxy);
+    const uint32_t r = (uint32_t)((int64_t)c - (int64_t)q.z * P.nxy);
     q.y = (int)fdiv(r, dnx);
     q.x = (int)(r - (uint32_t)q.y * (uint32_t)P.nx);
     const bool mv = WALLS && P.moving_any && touches_moving(P, q.x, q.y, q.z);
     R f[15];
-    load_pre<R, S, WALLS>(P, K, first != 0, fin, c, q, (mv && !first) ? rho_buf[c] : R(0), f);
+    load_pre<R, S, WALLS, I>(P, K, first != 0, fin, c, q, (mv && !first) ? rho_buf[c] : R(0), f);
     R rho, ux, uy, uz;
     collide<R, DEV>(K, f, F[c], F[V + c], F[2 * V + c], rho, ux, uy, uz);
 #pragma unroll

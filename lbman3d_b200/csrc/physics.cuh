@@ -81,23 +81,27 @@ __device__ __forceinline__ R v_ghost(const SimParams& P, const Phys<R>& K, int f
     return R(2.0) * wall - vb;
 }
 
-// VelocityAxisGradient (src/boundary_handler.h:157-163).
-template <class R>
+// VelocityAxisGradient (src/boundary_handler.h:157-163); HALF = false
+// returns the unhalved difference.
+template <class R, bool HALF = true>
 __device__ __forceinline__ R v_grad(const SimParams& P, const Phys<R>& K, const VRule& r, int comp, R m,
                                     R c, R p, bool normal) {
     if (r.m_clamp) m = c;
     if (r.p_clamp) p = c;
     if (r.m_wall) m = v_ghost<R>(P, K, r.lo, comp, c, normal);
     if (r.p_wall) p = v_ghost<R>(P, K, r.hi, comp, c, normal);
-    return R(0.5) * (p - m);
+    return HALF ? R(0.5) * (p - m) : (p - m);
 }
 
-template <class R>
+// HALF = false keeps the first differences unhalved (2x the centred
+// difference), for the FP32 right-hand side that folds the 1/2 into its
+// coefficients.
+template <class R, bool HALF = true>
 __device__ __forceinline__ QD<R> q_derivs(R xm, R xp, R ym, R yp, R zm, R zp, R c) {
     QD<R> d;
-    d.dx = R(0.5) * (xp - xm);
-    d.dy = R(0.5) * (yp - ym);
-    d.dz = R(0.5) * (zp - zm);
+    d.dx = HALF ? R(0.5) * (xp - xm) : (xp - xm);
+    d.dy = HALF ? R(0.5) * (yp - ym) : (yp - ym);
+    d.dz = HALF ? R(0.5) * (zp - zm) : (zp - zm);
     d.lap = (xm + xp + ym + yp + zm + zp) - R(6.0) * c;
     d.d2x = (xm + xp) - R(2.0) * c;
     d.d2y = (ym + yp) - R(2.0) * c;
@@ -128,18 +132,9 @@ __device__ __forceinline__ R adv_deriv(R ux, R uy, R uz, const QD<R>& d) {
 // PointwiseStepAndSetupBodyForce (src/model.h:102-342): Q_new, Sigma, tau and
 // the Ericksen force -H:grad Q at one cell.
 template <class R, bool UPWIND>
-__device__ __forceinline__ void pointwise_q_mat(const Phys<R>& K, const R Q[5], R ux, R uy, R uz,
-                                                const QD<R> d[5], const GradU<R>& g, R qn[5], R sig[5],
-                                                R tau[3], R eric[3]);
-
-template <class R, bool UPWIND>
 __device__ __forceinline__ void pointwise_q(const Phys<R>& K, const R Q[5], R ux, R uy, R uz,
                                             const QD<R> d[5], const GradU<R>& g, R qn[5], R sig[5],
                                             R tau[3], R eric[3]) {
-    if constexpr (sizeof(R) == 4) {
-        pointwise_q_mat<R, UPWIND>(K, Q, ux, uy, uz, d, g, qn, sig, tau, eric);
-        return;
-    }
     const R A = K.A, B = K.B, C = K.C, L = K.L, LAMBDA = K.LAMBDA, GAMMA = K.GAMMA, DT = K.DT;
     const R Qxx = Q[0], Qxy = Q[1], Qxz = Q[2], Qyy = Q[3], Qyz = Q[4];
 
@@ -231,13 +226,15 @@ __device__ __forceinline__ void pointwise_q(const Phys<R>& K, const R Q[5], R ux
     qn[4] = Qyz + DT * (adv_yz + cor_yz + LAMBDA * (k23 * Eyz + aln2_yz + aln3_yz) + GAMMA * Hyz);
 }
 
-// The same right-hand side for the FP32 instantiations, with the products of
-// two symmetric traceless tensors formed once as full matrices: for
-// M = Q E, QE + EQ = M + M^T; for N = Q H, QH + HQ = N + N^T and
-// tau = QH - HQ = N - N^T (HQ = (QH)^T), and tr = sum of the diagonal.  That
-// takes about 40 fewer operations per point than the reference's term-by-term
-// expansion (which the FP64 path keeps for bitwise parity); the values agree
-// to rounding.
+// The same right-hand side for the FP32 instantiations, with less arithmetic
+// (the values agree with the reference's term-by-term expansion, which the
+// FP64 path keeps for bitwise parity, to rounding):
+//  * d[k].dx/dy/dz and g are the UNHALVED first differences (2x the centred
+//    differences); the 1/2 is folded into the coefficients that use them;
+//  * co-rotation and alignment together, (WQ - QW) + LAMBDA (QE + EQ), are
+//    QB + (QB)^T with B = LAMBDA E - W (Q symmetric, W antisymmetric), and
+//    tr(QB) = LAMBDA tr(QE);
+//  * for N = QH, QH + HQ = N + N^T and tau = QH - HQ = N - N^T.
 template <class R, bool UPWIND>
 __device__ __forceinline__ void pointwise_q_mat(const Phys<R>& K, const R Q[5], R ux, R uy, R uz,
                                                 const QD<R> d[5], const GradU<R>& g, R qn[5], R sig[5],
@@ -250,34 +247,40 @@ __device__ __forceinline__ void pointwise_q_mat(const Phys<R>& K, const R Q[5], 
     // rhs_k: advection + co-rotation + LAMBDA (alignment), per component.
     R rhs[5];
 #pragma unroll
-    for (int k = 0; k < 5; ++k) rhs[k] = -adv_deriv<R, UPWIND>(ux, uy, uz, d[k]);
+    for (int k = 0; k < 5; ++k) {
+        R t = ux * d[k].dx + uy * d[k].dy + uz * d[k].dz;
+        if (UPWIND) {
+            const R ax = ux < R(0.0) ? -ux : ux, ay = uy < R(0.0) ? -uy : uy, az = uz < R(0.0) ? -uz : uz;
+            t = t - (ax * d[k].d2x + ay * d[k].d2y + az * d[k].d2z);
+        }
+        rhs[k] = R(-0.5) * t;
+    }
     {
-        const R Exx = g.ux_x, Eyy = g.uy_y, Ezz = -(Exx + Eyy);
-        const R Exy = R(0.5) * (g.ux_y + g.uy_x);
-        const R Exz = R(0.5) * (g.ux_z + g.uz_x);
-        const R Eyz = R(0.5) * (g.uy_z + g.uz_y);
-        const R Wxy = R(0.5) * (g.ux_y - g.uy_x);
-        const R Wxz = R(0.5) * (g.ux_z - g.uz_x);
-        const R Wyz = R(0.5) * (g.uy_z - g.uz_y);
-        rhs[0] += R(2.0) * (b * Wxy + c * Wxz);
-        rhs[1] += -a * Wxy + c * Wyz + e * Wxy + h * Wxz;
-        rhs[2] += R(-2.0) * a * Wxz - b * Wyz - e * Wxz + h * Wxy;
-        rhs[3] += R(2.0) * (-b * Wxy + h * Wyz);
-        rhs[4] += -a * Wyz - b * Wxz - c * Wxy - R(2.0) * e * Wyz;
-        // M = Q E
-        const R Mxx = a * Exx + b * Exy + c * Exz, Myy = b * Exy + e * Eyy + h * Eyz;
-        const R Mzz = c * Exz + h * Eyz + zz * Ezz;
-        const R trQE = Mxx + Myy + Mzz;
-        const R m2 = R(-2.0) * trQE;  // aln3 = -2 tr(QE) Q
-        const R kt = k23 * trQE;
-        rhs[0] += LAMBDA * (k23 * Exx + (R(2.0) * Mxx - kt) + m2 * a);
-        rhs[3] += LAMBDA * (k23 * Eyy + (R(2.0) * Myy - kt) + m2 * e);
-        const R Mxy = a * Exy + b * Eyy + c * Eyz, Myx = b * Exx + e * Exy + h * Exz;
-        rhs[1] += LAMBDA * (k23 * Exy + (Mxy + Myx) + m2 * b);
-        const R Mxz = a * Exz + b * Eyz + c * Ezz, Mzx = c * Exx + h * Exy + zz * Exz;
-        rhs[2] += LAMBDA * (k23 * Exz + (Mxz + Mzx) + m2 * c);
-        const R Myz = b * Exz + e * Eyz + h * Ezz, Mzy = c * Exy + h * Eyy + zz * Eyz;
-        rhs[4] += LAMBDA * (k23 * Eyz + (Myz + Mzy) + m2 * h);
+        const R Exx = R(0.5) * g.ux_x, Eyy = R(0.5) * g.uy_y;
+        const R Exy = R(0.25) * (g.ux_y + g.uy_x);
+        const R Exz = R(0.25) * (g.ux_z + g.uz_x);
+        const R Eyz = R(0.25) * (g.uy_z + g.uz_y);
+        const R Wxy = R(0.25) * (g.ux_y - g.uy_x);
+        const R Wxz = R(0.25) * (g.ux_z - g.uz_x);
+        const R Wyz = R(0.25) * (g.uy_z - g.uz_y);
+        const R Bxx = LAMBDA * Exx, Byy = LAMBDA * Eyy, Bzz = -(Bxx + Byy);
+        const R Bxy = LAMBDA * Exy - Wxy, Byx = LAMBDA * Exy + Wxy;
+        const R Bxz = LAMBDA * Exz - Wxz, Bzx = LAMBDA * Exz + Wxz;
+        const R Byz = LAMBDA * Eyz - Wyz, Bzy = LAMBDA * Eyz + Wyz;
+        // N = Q B
+        const R Nxx = a * Bxx + b * Byx + c * Bzx, Nyy = b * Bxy + e * Byy + h * Bzy;
+        const R Nzz = c * Bxz + h * Byz + zz * Bzz;
+        const R T = Nxx + Nyy + Nzz;  // LAMBDA tr(QE)
+        const R kT = k23 * T, m2 = R(-2.0) * T;
+        const R lk = LAMBDA * k23;
+        rhs[0] += (R(2.0) * Nxx - kT) + lk * Exx + m2 * a;
+        rhs[3] += (R(2.0) * Nyy - kT) + lk * Eyy + m2 * e;
+        const R Nxy = a * Bxy + b * Byy + c * Bzy, Nyx = b * Bxx + e * Byx + h * Bzx;
+        rhs[1] += (Nxy + Nyx) + lk * Exy + m2 * b;
+        const R Nxz = a * Bxz + b * Byz + c * Bzz, Nzx = c * Bxx + h * Byx + zz * Bzx;
+        rhs[2] += (Nxz + Nzx) + lk * Exz + m2 * c;
+        const R Nyz = b * Bxz + e * Byz + h * Bzz, Nzy = c * Bxy + h * Byy + zz * Bzy;
+        rhs[4] += (Nyz + Nzy) + lk * Eyz + m2 * h;
     }
 
     R H[5];
@@ -293,12 +296,13 @@ __device__ __forceinline__ void pointwise_q_mat(const Phys<R>& K, const R Q[5], 
     }
     const R Hxx = H[0], Hxy = H[1], Hxz = H[2], Hyy = H[3], Hyz = H[4], Hzz = -(Hxx + Hyy);
 
-    eric[0] = R(-2.0) * (Hxx * d[0].dx + Hxy * d[1].dx + Hxz * d[2].dx + Hyy * d[3].dx + Hyz * d[4].dx) -
-              Hxx * d[3].dx - Hyy * d[0].dx;
-    eric[1] = R(-2.0) * (Hxx * d[0].dy + Hxy * d[1].dy + Hxz * d[2].dy + Hyy * d[3].dy + Hyz * d[4].dy) -
-              Hxx * d[3].dy - Hyy * d[0].dy;
-    eric[2] = R(-2.0) * (Hxx * d[0].dz + Hxy * d[1].dz + Hxz * d[2].dz + Hyy * d[3].dz + Hyz * d[4].dz) -
-              Hxx * d[3].dz - Hyy * d[0].dz;
+    // -H : grad Q with the doubled differences: -2 sum_k H_k d_k - (Hxx d3 + Hyy d0)
+    eric[0] = -(Hxx * d[0].dx + Hxy * d[1].dx + Hxz * d[2].dx + Hyy * d[3].dx + Hyz * d[4].dx) -
+              R(0.5) * (Hxx * d[3].dx + Hyy * d[0].dx);
+    eric[1] = -(Hxx * d[0].dy + Hxy * d[1].dy + Hxz * d[2].dy + Hyy * d[3].dy + Hyz * d[4].dy) -
+              R(0.5) * (Hxx * d[3].dy + Hyy * d[0].dy);
+    eric[2] = -(Hxx * d[0].dz + Hxy * d[1].dz + Hxz * d[2].dz + Hyy * d[3].dz + Hyz * d[4].dz) -
+              R(0.5) * (Hxx * d[3].dz + Hyy * d[0].dz);
 
 #pragma unroll
     for (int k = 0; k < 5; ++k) qn[k] = Q[k] + DT * (rhs[k] + GAMMA * H[k]);

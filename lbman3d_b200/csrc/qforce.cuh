@@ -258,23 +258,25 @@ __device__ __forceinline__ void qf_compute_plane(const SimParams& P, const Phys<
         if (G.wx) q_apply<R>(qx, K, k, c, xm, xp);
         if (G.wy) q_apply<R>(qy, K, k, c, ym, yp);
         if (G.wz) q_apply<R>(qz, K, k, c, zm, zp);
-        d[k] = q_derivs<R>(xm, xp, ym, yp, zm, zp, c);
+        d[k] = q_derivs<R, !ST::COMB>(xm, xp, ym, yp, zm, zp, c);
         Q[k] = c;
     }
     const R* uc[3] = {Qc + 5 * NQU, Qc + 6 * NQU, Qc + 7 * NQU};
     const R u0[3] = {uc[0][up], uc[1][up], uc[2][up]};
     // (component, axis) pairs of the stored gradient: ux_x ux_y ux_z uy_x uy_y uy_z uz_x uz_y
+    // FP32 (COMB) keeps the differences unhalved; pointwise_q_mat folds the 1/2.
+    constexpr R HS = ST::COMB ? R(1.0) : R(0.5);
     R gr[8];
 #pragma unroll
     for (int comp = 0; comp < 3; ++comp) {
         const R c = u0[comp];
         const R xm = uc[comp][up - 1], xp = uc[comp][up + 1];
         const R ym = uc[comp][up - UX], yp = uc[comp][up + UX];
-        gr[comp * 3 + 0] = G.wx ? v_grad<R>(P, K, vx, comp, xm, c, xp, comp == 0) : R(0.5) * (xp - xm);
-        gr[comp * 3 + 1] = G.wy ? v_grad<R>(P, K, vy, comp, ym, c, yp, comp == 1) : R(0.5) * (yp - ym);
+        gr[comp * 3 + 0] = G.wx ? v_grad<R, !ST::COMB>(P, K, vx, comp, xm, c, xp, comp == 0) : HS * (xp - xm);
+        gr[comp * 3 + 1] = G.wy ? v_grad<R, !ST::COMB>(P, K, vy, comp, ym, c, yp, comp == 1) : HS * (yp - ym);
         if (comp < 2) {
             const R zm = Qm[(5 + comp) * NQU + up], zp = Qp[(5 + comp) * NQU + up];
-            gr[comp * 3 + 2] = G.wz ? v_grad<R>(P, K, vz, comp, zm, c, zp, false) : R(0.5) * (zp - zm);
+            gr[comp * 3 + 2] = G.wz ? v_grad<R, !ST::COMB>(P, K, vz, comp, zm, c, zp, false) : HS * (zp - zm);
         }
     }
     GradU<R> g;
@@ -282,7 +284,10 @@ __device__ __forceinline__ void qf_compute_plane(const SimParams& P, const Phys<
     g.uy_x = gr[3]; g.uy_y = gr[4]; g.uy_z = gr[5];
     g.uz_x = gr[6]; g.uz_y = gr[7];
     R sg[5], ta[3];
-    pointwise_q<R, UPWIND>(K, Q, u0[0], u0[1], u0[2], d, g, qn, sg, ta, er);
+    if constexpr (ST::COMB)
+        pointwise_q_mat<R, UPWIND>(K, Q, u0[0], u0[1], u0[2], d, g, qn, sg, ta, er);
+    else
+        pointwise_q<R, UPWIND>(K, Q, u0[0], u0[1], u0[2], d, g, qn, sg, ta, er);
     if constexpr (ST::COMB) {
         // Row stress Pi_ab = Sigma_ab + tau_ab - ALPHA Q_new_ab (tau_ba = -tau_ab),
         // grouped by the axis b it is differentiated along (f_a = d_b Pi_ab).
