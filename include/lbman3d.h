@@ -38,7 +38,7 @@ extern "C" {
 #define LBMAN_ERR_DIVERGED 3    /* NaN in the global mass or momentum            */
 #define LBMAN_ERR_TIMEOUT 4     /* a bounded device wait gave up                 */
 #define LBMAN_ERR_STATE 5       /* call out of order (e.g. step before upload)   */
-#define LBMAN_ERR_UNSUPPORTED 6 /* configuration this build does not implement   */
+#define LBMAN_ERR_UNSUPPORTED 6 /* configuration this library does not implement */
 #define LBMAN_ERR_NOMEM 7       /* device allocation failed                      */
 
 /* Q-tensor wall tags (src/boundary.h:31-42). */

@@ -1,5 +1,5 @@
 """Closure experiment: train the coarse-grid closure on box-filtered fine runs
-and judge it against a held-out fine run and against the plain coarse solver.
+and measure it against a held-out fine run and against the plain coarse solver.
 
     python -m lbman3d_b200.closure_experiment [--fine 256] [--factor 4] ...
 
@@ -7,7 +7,7 @@ Fine runs: FullyPeriodic, FP32, seeded random director (S0 = equilibrium
 order, 1e-3 Gaussian), zeta = ALPHA.  Every ``factor`` fine steps the fine
 state is box-filtered onto the coarse grid (one coarse step = ``factor``
 fine steps, coarse parameters from closure.coarse_params).  Training pairs
-come from the training seeds; the held-out seed is the judge:
+come from the training seeds; the held-out seed is the yardstick:
 
 * short-time error: relative L2 error of coarse Q and u against the
   filtered fine run after n coarse steps from the same filtered start, for

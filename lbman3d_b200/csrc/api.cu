@@ -350,7 +350,7 @@ int lbman_create(const lbman_config* cfg, lbman_solver** out) {
     cudaDeviceProp prop;
     if (cudaGetDeviceProperties(&prop, s->device) != cudaSuccess)
         return bail(fail(LBMAN_ERR_CUDA, "cudaGetDeviceProperties failed"));
-    if (prop.major < 10) return bail(fail(LBMAN_ERR_UNSUPPORTED, "this build targets sm_100a (B200); device is sm_%d%d", prop.major, prop.minor));
+    if (prop.major < 10) return bail(fail(LBMAN_ERR_UNSUPPORTED, "this library targets sm_100a (B200); device is sm_%d%d", prop.major, prop.minor));
     s->num_sms = prop.multiProcessorCount;
 
     build_sim_params(*cfg, s->P);

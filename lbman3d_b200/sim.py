@@ -9,7 +9,7 @@ frame export and the main / benchmark loops (src/main.cc, src/benchmark.cc).
 Log lines keep the reference's wording and number format (C++ std::format
 defaults, restated by ``cxx_format``) so tools that parse lbm.log -- the
 reference's monitor.py among them -- read them unchanged.  Frames: the
-reference writes VTKHDF through HDF5, which this build does not link; each
+reference writes VTKHDF through HDF5, which this library does not link; each
 frame is instead one raw little-endian file (``frame_{k:06d}.bin``) with a
 JSON header beside it listing the arrays, their dtype, shape ([nz, ny, nx]
 point data, the VTKHDF ordering) and byte offset: rho, velocity (3),

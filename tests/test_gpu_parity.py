@@ -5,7 +5,7 @@
   and the fused one-kernel step).
 * Larger seeded boxes against the CPU oracle: bitwise in FP64; FP32 and FP16
   deviation storage within stated relative max-norm bounds.
-* The north_star gate: per-field max relative error max|a-b|/max|b| on rho,
+* The FP64 error gate: per-field max relative error max|a-b|/max|b| on rho,
   u and Q of at most 1e-12 after one step and 1e-9 after 100 steps (FP64).
 """
 import numpy as np
@@ -94,7 +94,7 @@ def test_fp64_bitwise_vs_oracle_larger_boxes(bc, grid, upwind, kernels):
             np.testing.assert_array_equal(a[f], b[f], err_msg=f"{bc} {f}")
 
 
-def test_north_star_gate_fp64_periodic_32():
+def test_fp64_error_gate_periodic_32():
     """FullyPeriodic 32^3, params.h defaults, seeded random director: <=1e-12
     after 1 step and <=1e-9 after 100 steps against the CPU oracle."""
     from cases import BC
