@@ -151,6 +151,43 @@ __device__ __forceinline__ void gather(const SimParams& P, const Phys<R>& K, con
     }
 }
 
+// BGK relaxation with Guo forcing for the FP32 instantiations, by opposite
+// pairs (j, opp(j)), e_opp = -e_j: with ue = e_j.u and eF = e_j.F, the
+// equilibrium and forcing terms split into a part even in (ue, eF) and an
+// odd part that flips sign, so one evaluation serves both directions:
+//   f_j   <- om f_j   + G + H,   f_opp <- om f_opp + G - H,
+//   G = omp w (s + rho (4.5 ue^2 - 1.5 u^2)) + DT omf w (9 ue eF - 3 u.F)
+//       (DEV; plain storage has w rho (1 + ...) in place of w (s + rho ...)),
+//   H = omp w rho 3 ue + DT omf w 3 eF.
+// The same values as the direction-by-direction form (which the FP64 path
+// keeps for bitwise parity) up to rounding.
+template <class R, bool DEV>
+__device__ __forceinline__ void relax_pairs(R om, R omp, R omf, R DT, R s, R rho, R ux, R uy, R uz, R Fx, R Fy,
+                                            R Fz, R uF, R u2, R f[15]) {
+    const R t = R(1.5) * u2, m3uF = R(-3.0) * uF, r3 = R(3.0) * rho;
+    {
+        const R w = w_<R>(0);
+        const R feq = DEV ? w * (s - rho * t) : w * rho * (R(1.0) - t);
+        f[0] = om * f[0] + (omp * feq + DT * omf * w * m3uF);
+    }
+#pragma unroll
+    for (int j = 1; j < 15; ++j) {
+        if (opp_(j) < j) continue;
+        const int o = opp_(j);
+        const R w = w_<R>(j);
+        const R cw = omp * w, fw = DT * omf * w;
+        const R ue = edot<R>(ex_(j), ey_(j), ez_(j), ux, uy, uz);
+        const R eF = edot<R>(ex_(j), ey_(j), ez_(j), Fx, Fy, Fz);
+        const R A = R(4.5) * ue * ue - t;
+        const R even = DEV ? s + rho * A : rho * (R(1.0) + A);
+        const R G = cw * even + fw * (R(9.0) * ue * eF + m3uF);
+        const R H = cw * (r3 * ue) + fw * (R(3.0) * eF);
+        const R fj = f[j], fo = f[o];
+        f[j] = om * fj + (G + H);
+        f[o] = om * fo + (G - H);
+    }
+}
+
 // Moments, equilibrium, Guo forcing and BGK relaxation of one cell
 // (src/physics_helpers.h:69-129); f is overwritten with f*.
 template <class R, bool DEV>
@@ -183,6 +220,10 @@ __device__ __forceinline__ void collide(const Phys<R>& K, R f[15], R Fx, R Fy, R
     const R uF = ux * Fx + uy * Fy + uz * Fz;
     const R u2 = ux * ux + uy * uy + uz * uz;
     const R om = K.omega, omp = K.omega_prime, omf = K.omega_forcing;
+    if constexpr (sizeof(R) == 4) {
+        relax_pairs<R, DEV>(om, omp, omf, DT, s, rho, ux, uy, uz, Fx, Fy, Fz, uF, u2, f);
+        return;
+    }
 #pragma unroll
     for (int j = 0; j < 15; ++j) {
         const R w = w_<R>(j);

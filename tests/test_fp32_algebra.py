@@ -1,4 +1,4 @@
-"""The FP32 Q-stage right-hand side (csrc/physics.cuh pointwise_q_mat) is an
+"""The FP32 arithmetic rearrangements.  The Q-stage right-hand side (csrc/physics.cuh pointwise_q_mat) is an
 algebraic rearrangement of the reference's term-by-term expansion
 (pointwise_q, src/model.h:102-342).  Compiled here as host C++ in double
 precision, the two must agree to rounding on random states."""
@@ -17,5 +17,18 @@ def test_fp32_rhs_matches_reference_form(tmp_path):
     exe = str(tmp_path / "algebra_check")
     subprocess.run(["g++", "-std=c++17", "-O1", "-I", os.path.join(HERE, "host", "stub"), "-I", CSRC,
                     os.path.join(HERE, "host", "algebra_check.cpp"), "-o", exe], check=True)
+    r = subprocess.run([exe], capture_output=True, text=True)
+    assert r.returncode == 0, r.stdout + r.stderr
+
+
+@pytest.mark.skipif(shutil.which("g++") is None, reason="needs g++")
+def test_fp32_paired_relaxation_matches_reference_form(tmp_path):
+    """The FP32 BGK + Guo relaxation by opposite direction pairs
+    (csrc/lbm.cuh relax_pairs) against the direction-by-direction form of the
+    reference (src/physics_helpers.h:69-129), in double, with and without
+    deviation storage."""
+    exe = str(tmp_path / "collide_check")
+    subprocess.run(["g++", "-std=c++17", "-O1", "-I", os.path.join(HERE, "host", "stub"), "-I", CSRC,
+                    os.path.join(HERE, "host", "collide_check.cpp"), "-o", exe], check=True)
     r = subprocess.run([exe], capture_output=True, text=True)
     assert r.returncode == 0, r.stdout + r.stderr
