@@ -194,16 +194,32 @@ template <class R, bool DEV>
 __device__ __forceinline__ void collide(const Phys<R>& K, R f[15], R Fx, R Fy, R Fz, R& rho, R& ux,
                                         R& uy, R& uz) {
     const R DT = K.DT;
-    R s = f[0];
+    R s, jx = R(0), jy = R(0), jz = R(0);
+    if constexpr (sizeof(R) == 4) {
+        // FP32: by opposite pairs, s = f0 + sum (f_j + f_opp) and
+        // j = sum e_j (f_j - f_opp) -- shorter dependency chains.
+        s = f[0];
+        bool hx = false, hy = false, hz = false;
 #pragma unroll
-    for (int j = 1; j < 15; ++j) s = s + f[j];
-    R jx = R(0), jy = R(0), jz = R(0);
-    bool hx = false, hy = false, hz = false;
+        for (int j = 1; j < 15; ++j) {
+            if (opp_(j) < j) continue;
+            const R p = f[j] + f[opp_(j)], m = f[j] - f[opp_(j)];
+            s = s + p;
+            if (ex_(j)) { const R t = sgn_term(ex_(j), m); jx = hx ? jx + t : t; hx = true; }
+            if (ey_(j)) { const R t = sgn_term(ey_(j), m); jy = hy ? jy + t : t; hy = true; }
+            if (ez_(j)) { const R t = sgn_term(ez_(j), m); jz = hz ? jz + t : t; hz = true; }
+        }
+    } else {  // the reference's summation order, for bitwise FP64 parity
+        s = f[0];
 #pragma unroll
-    for (int j = 0; j < 15; ++j) {
-        if (ex_(j)) { const R t = sgn_term(ex_(j), f[j]); jx = hx ? jx + t : t; hx = true; }
-        if (ey_(j)) { const R t = sgn_term(ey_(j), f[j]); jy = hy ? jy + t : t; hy = true; }
-        if (ez_(j)) { const R t = sgn_term(ez_(j), f[j]); jz = hz ? jz + t : t; hz = true; }
+        for (int j = 1; j < 15; ++j) s = s + f[j];
+        bool hx = false, hy = false, hz = false;
+#pragma unroll
+        for (int j = 0; j < 15; ++j) {
+            if (ex_(j)) { const R t = sgn_term(ex_(j), f[j]); jx = hx ? jx + t : t; hx = true; }
+            if (ey_(j)) { const R t = sgn_term(ey_(j), f[j]); jy = hy ? jy + t : t; hy = true; }
+            if (ez_(j)) { const R t = sgn_term(ez_(j), f[j]); jz = hz ? jz + t : t; hz = true; }
+        }
     }
     const R rho0 = K.kDensity;
     rho = DEV ? rho0 + s : s;  // DEV: s is the density deviation
