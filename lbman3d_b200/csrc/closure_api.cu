@@ -255,7 +255,8 @@ int check_err(lbman_closure* c) {
     int h = 0;
     CL_CUDA(cudaMemcpy(&h, c->err, sizeof(int), cudaMemcpyDeviceToHost));
     if (h) {
-        cudaMemset(c->err, 0, sizeof(int));
+        cudaMemsetAsync(c->err, 0, sizeof(int), c->stream);
+        cudaStreamSynchronize(c->stream);
         return failc(LBMAN_ERR_TIMEOUT, "closure: a tensor-core wait timed out");
     }
     return LBMAN_OK;
@@ -345,16 +346,20 @@ int lbman_closure_create(int device, int nx, int ny, int nz, uint64_t seed, lbma
                 }
         for (int co = 0; co < d.real_cout; ++co) hm[b_off(l) + co] = 1.0f;
     }
-    cudaMemcpy(c->p, hp.data(), P, cudaMemcpyHostToDevice);
-    cudaMemcpy(c->mask, hm.data(), P, cudaMemcpyHostToDevice);
-    cudaMemset(c->m, 0, P);
-    cudaMemset(c->v, 0, P);
-    cudaMemset(c->g, 0, P);
-    cudaMemset(c->err, 0, sizeof(int));
+    // Every upload and clear goes on the closure's own (non-blocking) stream,
+    // so the kernels queued after it see the data: a plain cudaMemcpy from
+    // pageable memory may return before its DMA lands, and the legacy stream
+    // does not order work on a non-blocking one.
+    cudaMemcpyAsync(c->p, hp.data(), P, cudaMemcpyHostToDevice, c->stream);
+    cudaMemcpyAsync(c->mask, hm.data(), P, cudaMemcpyHostToDevice, c->stream);
+    cudaMemsetAsync(c->m, 0, P, c->stream);
+    cudaMemsetAsync(c->v, 0, P, c->stream);
+    cudaMemsetAsync(c->g, 0, P, c->stream);
+    cudaMemsetAsync(c->err, 0, sizeof(int), c->stream);
     // B images are fully rewritten by pack; zero them once so padding is 0
     for (int l = 0; l < 4; ++l) {
-        cudaMemset(c->fimg[l], 0, cl::bimg_bytes(kLayers[l].cin, kLayers[l].cout));
-        if (l > 0) cudaMemset(c->bimg[l], 0, cl::bimg_bytes(kLayers[l].cout, kLayers[l].cin));
+        cudaMemsetAsync(c->fimg[l], 0, cl::bimg_bytes(kLayers[l].cin, kLayers[l].cout), c->stream);
+        if (l > 0) cudaMemsetAsync(c->bimg[l], 0, cl::bimg_bytes(kLayers[l].cout, kLayers[l].cin), c->stream);
     }
     int s = pack(c, c->stream);
     if (s == LBMAN_OK) s = upload_scales(c);
@@ -398,7 +403,7 @@ int lbman_closure_set_params(lbman_closure* c, const float* p) {
     std::vector<float> hm(kNParams), hp(p, p + kNParams);
     CL_CUDA(cudaMemcpy(hm.data(), c->mask, kNParams * sizeof(float), cudaMemcpyDeviceToHost));
     for (int i = 0; i < kNParams; ++i) hp[i] *= hm[i];
-    CL_CUDA(cudaMemcpy(c->p, hp.data(), kNParams * sizeof(float), cudaMemcpyHostToDevice));
+    CL_CUDA(cudaMemcpyAsync(c->p, hp.data(), kNParams * sizeof(float), cudaMemcpyHostToDevice, c->stream));
     CL_TRY(pack(c, c->stream));
     CL_CUDA(cudaStreamSynchronize(c->stream));
     return LBMAN_OK;
@@ -432,7 +437,8 @@ int lbman_closure_forward(lbman_closure* c, const float* feat9, float* out8) {
     float* dx = nullptr;
     CL_CUDA(cudaMalloc(&dx, 9 * V * sizeof(float)));
     int s = LBMAN_OK;
-    if (cudaMemcpy(dx, feat9, 9 * V * sizeof(float), cudaMemcpyHostToDevice) != cudaSuccess) s = LBMAN_ERR_CUDA;
+    if (cudaMemcpyAsync(dx, feat9, 9 * V * sizeof(float), cudaMemcpyHostToDevice, c->stream) != cudaSuccess)
+        s = LBMAN_ERR_CUDA;
     if (s == LBMAN_OK) s = features(c, c->stream, dx, dx + V, dx + 4 * V);
     if (s == LBMAN_OK) s = forward(c, c->stream);
     if (s == LBMAN_OK && cudaStreamSynchronize(c->stream) != cudaSuccess) s = LBMAN_ERR_CUDA;
@@ -457,8 +463,8 @@ int lbman_closure_gradient(lbman_closure* c, const float* feat9, const float* ta
     int s = LBMAN_OK;
     if (cudaMalloc(&dt, 8 * V * sizeof(float)) != cudaSuccess || cudaMalloc(&dl, sizeof(double)) != cudaSuccess)
         s = LBMAN_ERR_NOMEM;
-    if (s == LBMAN_OK && (cudaMemcpy(dx, feat9, 9 * V * 4, cudaMemcpyHostToDevice) != cudaSuccess ||
-                          cudaMemcpy(dt, target8, 8 * V * 4, cudaMemcpyHostToDevice) != cudaSuccess))
+    if (s == LBMAN_OK && (cudaMemcpyAsync(dx, feat9, 9 * V * 4, cudaMemcpyHostToDevice, c->stream) != cudaSuccess ||
+                          cudaMemcpyAsync(dt, target8, 8 * V * 4, cudaMemcpyHostToDevice, c->stream) != cudaSuccess))
         s = LBMAN_ERR_CUDA;
     if (s == LBMAN_OK) s = features(c, c->stream, dx, dx + V, dx + 4 * V);
     if (s == LBMAN_OK) s = forward(c, c->stream);

@@ -129,9 +129,13 @@ int build_work(lbman_ensemble* e) {
     e->lwork = nullptr;
     E_CUDA(cudaMalloc(&e->qwork, q.size() * sizeof(EnsQWork)));
     E_CUDA(cudaMalloc(&e->lwork, l.size() * sizeof(EnsLbmWork)));
-    E_CUDA(cudaMemcpy(e->qwork, q.data(), q.size() * sizeof(EnsQWork), cudaMemcpyHostToDevice));
-    E_CUDA(cudaMemcpy(e->lwork, l.data(), l.size() * sizeof(EnsLbmWork), cudaMemcpyHostToDevice));
-    E_CUDA(cudaMemcpy(e->dboxes, e->host.data(), e->n * sizeof(EnsBox), cudaMemcpyHostToDevice));
+    // On the ensemble's (non-blocking) stream and waited for: a plain
+    // cudaMemcpy from pageable memory may return before its DMA lands, and
+    // the legacy stream does not order the kernels queued on this one.
+    E_CUDA(cudaMemcpyAsync(e->qwork, q.data(), q.size() * sizeof(EnsQWork), cudaMemcpyHostToDevice, e->stream));
+    E_CUDA(cudaMemcpyAsync(e->lwork, l.data(), l.size() * sizeof(EnsLbmWork), cudaMemcpyHostToDevice, e->stream));
+    E_CUDA(cudaMemcpyAsync(e->dboxes, e->host.data(), e->n * sizeof(EnsBox), cudaMemcpyHostToDevice, e->stream));
+    E_CUDA(cudaStreamSynchronize(e->stream));
     e->nq = (int)q.size();
     e->nl = (int)l.size();
     const int bps = std::max(1, e->ops().blocks_per_sm(e->tcx, e->tcy, e->kernels == LBMAN_KERNELS_FUSED));

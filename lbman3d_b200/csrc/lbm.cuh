@@ -238,18 +238,18 @@ __device__ __forceinline__ void collide(const Phys<R>& K, R f[15], R Fx, R Fy, R
     const R om = K.omega, omp = K.omega_prime, omf = K.omega_forcing;
     if constexpr (sizeof(R) == 4) {
         relax_pairs<R, DEV>(om, omp, omf, DT, s, rho, ux, uy, uz, Fx, Fy, Fz, uF, u2, f);
-        return;
-    }
+    } else {
 #pragma unroll
-    for (int j = 0; j < 15; ++j) {
-        const R w = w_<R>(j);
-        const R ue = edot<R>(ex_(j), ey_(j), ez_(j), ux, uy, uz);
-        const R eF = edot<R>(ex_(j), ey_(j), ez_(j), Fx, Fy, Fz);
-        const R poly = R(1.0) + R(3.0) * ue + R(4.5) * ue * ue - R(1.5) * u2;
-        // DEV: f_eq - w rho0 = w (rho - rho0) + w rho (poly - 1)
-        const R feq = DEV ? w * (s + rho * (poly - R(1.0))) : w * rho * poly;
-        const R forcing = omf * w * (R(3.0) * eF - R(3.0) * uF + R(9.0) * ue * eF);
-        f[j] = om * f[j] + omp * feq + DT * forcing;
+        for (int j = 0; j < 15; ++j) {
+            const R w = w_<R>(j);
+            const R ue = edot<R>(ex_(j), ey_(j), ez_(j), ux, uy, uz);
+            const R eF = edot<R>(ex_(j), ey_(j), ez_(j), Fx, Fy, Fz);
+            const R poly = R(1.0) + R(3.0) * ue + R(4.5) * ue * ue - R(1.5) * u2;
+            // DEV: f_eq - w rho0 = w (rho - rho0) + w rho (poly - 1)
+            const R feq = DEV ? w * (s + rho * (poly - R(1.0))) : w * rho * poly;
+            const R forcing = omf * w * (R(3.0) * eF - R(3.0) * uF + R(9.0) * ue * eF);
+            f[j] = om * f[j] + omp * feq + DT * forcing;
+        }
     }
 }
 

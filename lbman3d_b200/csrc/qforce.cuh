@@ -228,12 +228,16 @@ __device__ __forceinline__ void narrow_walls(PointGeo& g, const AxisRule& qx, co
 
 // Beris-Edwards update of this thread's point in plane zb; results to the
 // ring slots of zb, Ericksen force to er, Q_new to qn.
-template <class TL, class R, bool UPWIND>
+// RM: which wall-rule code is compiled in -- 0 none, 1 the x axis only
+// (every point's y and z rules are off), 2 all axes as the flags say.
+template <class TL, class R, bool UPWIND, int RM>
 __device__ __forceinline__ void qf_compute_plane(const SimParams& P, const Phys<R>& K, const PointGeo& G,
                                                  const AxisRule& qx, const AxisRule& qy, const VRule& vx,
                                                  const VRule& vy, int z0, int zb, const R* QU, R* Bs,
                                                  R er[3], R qn[5]) {
     if (!G.hasB) return;
+    // wall rules compiled in and active in this warp, per axis
+    const bool rx = RM == 1 || (RM == 2 && G.wx), ry = RM == 2 && G.wy, rz = RM == 2 && G.wz;
     using ST = Stage<TL, R>;
     constexpr int NQU = ST::NQU, UX = ST::UX, NB = TL::NB;
     const R* Qc = QU + ring4(zb, z0) * 8 * NQU;
@@ -242,7 +246,7 @@ __device__ __forceinline__ void qf_compute_plane(const SimParams& P, const Phys<
     const int up = (G.lby + 1) * UX + G.lbx + ST::XO - 1;
     AxisRule qz;
     VRule vz;
-    if (G.wz) {
+    if (rz) {
         const int az = wrap_coord(zb, P.nz);
         qz = q_rule(P, 2, az, P.nz);
         vz = v_rule(P, 2, az, P.nz);
@@ -255,9 +259,9 @@ __device__ __forceinline__ void qf_compute_plane(const SimParams& P, const Phys<
         const R c = qc[up];
         R xm = qc[up - 1], xp = qc[up + 1], ym = qc[up - UX], yp = qc[up + UX];
         R zm = Qm[k * NQU + up], zp = Qp[k * NQU + up];
-        if (G.wx) q_apply<R>(qx, K, k, c, xm, xp);
-        if (G.wy) q_apply<R>(qy, K, k, c, ym, yp);
-        if (G.wz) q_apply<R>(qz, K, k, c, zm, zp);
+        if (rx) q_apply<R>(qx, K, k, c, xm, xp);
+        if (ry) q_apply<R>(qy, K, k, c, ym, yp);
+        if (rz) q_apply<R>(qz, K, k, c, zm, zp);
         d[k] = q_derivs<R, !ST::COMB>(xm, xp, ym, yp, zm, zp, c);
         Q[k] = c;
     }
@@ -272,11 +276,11 @@ __device__ __forceinline__ void qf_compute_plane(const SimParams& P, const Phys<
         const R c = u0[comp];
         const R xm = uc[comp][up - 1], xp = uc[comp][up + 1];
         const R ym = uc[comp][up - UX], yp = uc[comp][up + UX];
-        gr[comp * 3 + 0] = G.wx ? v_grad<R, !ST::COMB>(P, K, vx, comp, xm, c, xp, comp == 0) : HS * (xp - xm);
-        gr[comp * 3 + 1] = G.wy ? v_grad<R, !ST::COMB>(P, K, vy, comp, ym, c, yp, comp == 1) : HS * (yp - ym);
+        gr[comp * 3 + 0] = rx ? v_grad<R, !ST::COMB>(P, K, vx, comp, xm, c, xp, comp == 0) : HS * (xp - xm);
+        gr[comp * 3 + 1] = ry ? v_grad<R, !ST::COMB>(P, K, vy, comp, ym, c, yp, comp == 1) : HS * (yp - ym);
         if (comp < 2) {
             const R zm = Qm[(5 + comp) * NQU + up], zp = Qp[(5 + comp) * NQU + up];
-            gr[comp * 3 + 2] = G.wz ? v_grad<R, !ST::COMB>(P, K, vz, comp, zm, c, zp, false) : HS * (zp - zm);
+            gr[comp * 3 + 2] = rz ? v_grad<R, !ST::COMB>(P, K, vz, comp, zm, c, zp, false) : HS * (zp - zm);
         }
     }
     GradU<R> g;
@@ -330,23 +334,25 @@ __device__ __forceinline__ R anchor_delta(const AxisRule& r, const Phys<R>& K, i
 // Body force of this thread's tile cell in plane zc from the staged result
 // planes; out(cell, x, y, z, qn[5], F[3], u[3]) consumes it.  qc is the
 // cell's Q_new (kept in registers by the FP32 path).
-template <class TL, class R, class OutFn>
+template <class TL, class R, int RM, class OutFn>
 __device__ __forceinline__ void qf_force_cell(const SimParams& P, const Phys<R>& K, const PointGeo& G,
                                               const AxisRule& qx, const AxisRule& qy, int x0, int y0, int z0,
                                               int zc, const R* QU, const R* Bs, const R er[3], const R qc[5],
                                               OutFn&& out) {
     if (!G.isC) return;
+    // wall rules compiled in and active in this warp, per axis
+    const bool rx = RM == 1 || (RM == 2 && G.wx), ry = RM == 2 && G.wy, rz = RM == 2 && G.wz;
     using ST = Stage<TL, R>;
     constexpr int NB = TL::NB, BX = TL::BX;
     const int t = G.p;
     const int gx = x0 + G.lbx - 1, gy = y0 + G.lby - 1;
     AxisRule qz;
-    if (G.wz) qz = q_rule(P, 2, zc, P.nz);
+    if (rz) qz = q_rule(P, 2, zc, P.nz);
     // Sigma / tau differences with the Neumann/periodic index clamp QXoff
     // (src/offsets.h:59-83, used by PassiveStressDivergence).
-    const bool xmc = G.wx && gx == 0 && !P.qper[0], xpc = G.wx && gx == P.nx - 1 && !P.qper[1];
-    const bool ymc = G.wy && gy == 0 && !P.qper[2], ypc = G.wy && gy == P.ny - 1 && !P.qper[3];
-    const bool zmc = G.wz && zc == 0 && !P.qper[4], zpc = G.wz && zc == P.nz - 1 && !P.qper[5];
+    const bool xmc = rx && gx == 0 && !P.qper[0], xpc = rx && gx == P.nx - 1 && !P.qper[1];
+    const bool ymc = ry && gy == 0 && !P.qper[2], ypc = ry && gy == P.ny - 1 && !P.qper[3];
+    const bool zmc = rz && zc == 0 && !P.qper[4], zpc = rz && zc == P.nz - 1 && !P.qper[5];
     const R* U0 = QU + ring4(zc, z0) * 8 * ST::NQU;
     const int up = (G.lby + 1) * ST::UX + G.lbx + ST::XO - 1;
     const R u[3] = {U0[5 * ST::NQU + up], U0[6 * ST::NQU + up], U0[7 * ST::NQU + up]};
@@ -364,31 +370,31 @@ __device__ __forceinline__ void qf_force_cell(const SimParams& P, const Phys<R>&
             const R* py = Bxy + (3 + a) * NB;
             R xm = px[-1], xp = px[1], ym = py[-BX], yp = py[BX];
             R zm = Bzm[a * NB], zp = Bzp[a * NB];
-            if (G.wx) {
+            if (rx) {
                 if (xmc) xm = px[0];
                 if (xpc) xp = px[0];
             }
-            if (G.wy) {
+            if (ry) {
                 if (ymc) ym = py[0];
                 if (ypc) yp = py[0];
             }
-            if (G.wz) {
+            if (rz) {
                 if (zmc) zm = Bz0[a * NB];
                 if (zpc) zp = Bz0[a * NB];
             }
             f[a] = R(0.5) * (xp - xm) + R(0.5) * (yp - ym) + R(0.5) * (zp - zm);
         }
-        if (G.wx && (qx.m_ghost || qx.p_ghost)) {
+        if (rx && (qx.m_ghost || qx.p_ghost)) {
             f[0] += -K.ALPHA * anchor_delta<R>(qx, K, 0, qc[0]);
             f[1] += -K.ALPHA * anchor_delta<R>(qx, K, 1, qc[1]);
             f[2] += -K.ALPHA * anchor_delta<R>(qx, K, 2, qc[2]);
         }
-        if (G.wy && (qy.m_ghost || qy.p_ghost)) {
+        if (ry && (qy.m_ghost || qy.p_ghost)) {
             f[0] += -K.ALPHA * anchor_delta<R>(qy, K, 1, qc[1]);
             f[1] += -K.ALPHA * anchor_delta<R>(qy, K, 3, qc[3]);
             f[2] += -K.ALPHA * anchor_delta<R>(qy, K, 4, qc[4]);
         }
-        if (G.wz && (qz.m_ghost || qz.p_ghost)) {
+        if (rz && (qz.m_ghost || qz.p_ghost)) {
             f[0] += -K.ALPHA * anchor_delta<R>(qz, K, 2, qc[2]);
             f[1] += -K.ALPHA * anchor_delta<R>(qz, K, 4, qc[4]);
             f[2] += K.ALPHA * (anchor_delta<R>(qz, K, 0, qc[0]) + anchor_delta<R>(qz, K, 3, qc[3]));
@@ -411,9 +417,9 @@ __device__ __forceinline__ void qf_force_cell(const SimParams& P, const Phys<R>&
             qn[k] = c;
             R xm = b[t - 1], xp = b[t + 1], ym = b[t - BX], yp = b[t + BX];
             R zm = Bm[k * NB + t], zp = Bp[k * NB + t];
-            if (G.wx) q_apply<R>(qx, K, k, c, xm, xp);
-            if (G.wy) q_apply<R>(qy, K, k, c, ym, yp);
-            if (G.wz) q_apply<R>(qz, K, k, c, zm, zp);
+            if (rx) q_apply<R>(qx, K, k, c, xm, xp);
+            if (ry) q_apply<R>(qy, K, k, c, ym, yp);
+            if (rz) q_apply<R>(qz, K, k, c, zm, zp);
             dQ[k][0] = R(0.5) * (xp - xm);
             dQ[k][1] = R(0.5) * (yp - ym);
             dQ[k][2] = R(0.5) * (zp - zm);
@@ -460,8 +466,18 @@ __device__ __forceinline__ void qf_march(const SimParams& P, int x0, int y0, int
     for (int z = z0 - 2; z <= z0 + 1; ++z) qf_load_plane<TL>(P, x0, y0, z0, z, qin, uin, QU, vec, ps);
     cp_async_wait_all();
     __syncthreads();
-    qf_compute_plane<TL, R, UPWIND>(P, K, G, qx, qy, vx, vy, z0, z0 - 1, QU, Bs, er_next, qn_next);
-    qf_compute_plane<TL, R, UPWIND>(P, K, G, qx, qy, vx, vy, z0, z0, QU, Bs, er_cur, qn_cur);
+    // Warps none of whose points has a wall rule run the point update and
+    // the force with the rule code compiled out, warps with x rules only
+    // (the slit's wall columns) a copy without the y and z rule code; one
+    // warp-uniform choice per warp, made once per column segment.
+    const int rm = (G.wx || G.wy || G.wz) ? ((G.wy || G.wz) ? 2 : 1) : 0;
+    auto compute = [&](int zb, R er[3], R qn[5]) {
+        if (rm == 0) qf_compute_plane<TL, R, UPWIND, 0>(P, K, G, qx, qy, vx, vy, z0, zb, QU, Bs, er, qn);
+        else if (rm == 1) qf_compute_plane<TL, R, UPWIND, 1>(P, K, G, qx, qy, vx, vy, z0, zb, QU, Bs, er, qn);
+        else qf_compute_plane<TL, R, UPWIND, 2>(P, K, G, qx, qy, vx, vy, z0, zb, QU, Bs, er, qn);
+    };
+    compute(z0 - 1, er_next, qn_next);
+    compute(z0, er_cur, qn_cur);
     __syncthreads();  // the slot of z0-2 is free again
     qf_load_plane<TL>(P, x0, y0, z0, z0 + 2, qin, uin, QU, vec, ps);
     cp_async_wait_all();
@@ -469,11 +485,13 @@ __device__ __forceinline__ void qf_march(const SimParams& P, int x0, int y0, int
 #pragma unroll 1
     for (int zc = z0; zc < z1; ++zc) {
         if (zc + 1 < z1) qf_load_plane<TL>(P, x0, y0, z0, zc + 3, qin, uin, QU, vec, ps);
-        qf_compute_plane<TL, R, UPWIND>(P, K, G, qx, qy, vx, vy, z0, zc + 1, QU, Bs, er_next, qn_next);
+        compute(zc + 1, er_next, qn_next);
         // No barrier here: the force of plane zc reads its neighbours' results
         // of plane zc (written before the last barrier, in a slot that plane
         // zc + 1 does not use) and the z-ring only at its own point.
-        qf_force_cell<TL, R>(P, K, G, qx, qy, x0, y0, z0, zc, QU, Bs, er_cur, qn_cur, out);
+        if (rm == 0) qf_force_cell<TL, R, 0>(P, K, G, qx, qy, x0, y0, z0, zc, QU, Bs, er_cur, qn_cur, out);
+        else if (rm == 1) qf_force_cell<TL, R, 1>(P, K, G, qx, qy, x0, y0, z0, zc, QU, Bs, er_cur, qn_cur, out);
+        else qf_force_cell<TL, R, 2>(P, K, G, qx, qy, x0, y0, z0, zc, QU, Bs, er_cur, qn_cur, out);
 #pragma unroll
         for (int k = 0; k < 3; ++k) er_cur[k] = er_next[k];
 #pragma unroll
