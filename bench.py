@@ -377,7 +377,7 @@ def main():
     sim.set_stream(stream.cuda_stream)
     if a.kernels == "auto" and not tile:
         sim.init_seeded(1234, 0.5, 1e-3)
-        tuned = sim.autotune(steps_per_trial=3 if V > 5e7 else 10)
+        tuned = sim.autotune(steps_per_trial=8 if V > 5e7 else 10)
         config["autotuned"] = {k: tuned[k] for k in ("kernels", "tile_x", "tile_y", "zchunk", "trials")}
     sh = sim.shape()
     config["kernels"] = {1: "split", 2: "fused"}[sh["kernels"]]

@@ -126,8 +126,14 @@ __device__ __forceinline__ void gather(const SimParams& P, const Phys<R>& K, con
         // Source slot: the neighbour's j, or for a wall crossing this cell's
         // bi.  Only the index differs between the lanes, so a warp holding a
         // wall lane still issues one load per direction.
-        I src = j * V + c + off;
-        if (cx || cy || cz) src = (I)wall_source(P, j, cx, cy, cz, nullptr) * V + c;
+        // Written as selects (no branch), so the 15 loads stay one block.
+        const int ix = P.face[ex_(j) > 0 ? 0 : 1].ubc == U_SPECULAR ? spec_(0, j) : opp_(j);
+        const int iy = P.face[ey_(j) > 0 ? 2 : 3].ubc == U_SPECULAR ? spec_(1, j) : opp_(j);
+        const int iz = P.face[ez_(j) > 0 ? 4 : 5].ubc == U_SPECULAR ? spec_(2, j) : opp_(j);
+        int bi = cx ? ix : -1;
+        bi = (cy && iy >= bi) ? iy : bi;
+        bi = (cz && iz >= bi) ? iz : bi;
+        const I src = (cx || cy || cz) ? (I)bi * V + c : j * V + c + off;
         raw[j] = Store<S>::raw(fin + src);
     }
 #pragma unroll
