@@ -160,9 +160,10 @@ cudaError_t lbm(const SimParams& P, bool first, bool wr, const void* fin, void* 
                                  (R*)uout, wr ? 1 : 0);
     };
     const bool walls = !(P.uper[0] && P.uper[2] && P.uper[4]);
-    // 32-bit index arithmetic where every population offset fits in an int;
-    // measured on B200 it pays for FP16 storage (5-7%) and not for FP32/FP64.
-    if constexpr (sizeof(S) == 2) {
+    // 32-bit index arithmetic where every population offset fits in an int.
+    // Measured on B200 it pays for FP16 storage (5-7%), FP64 (2-4%) and the
+    // walled FP32 form (1%), and costs the periodic FP32 form 1-2%.
+    if (!(sizeof(S) == 4 && !walls)) {
         if (15 * P.V < ((int64_t)1 << 31)) {
             if (walls) launch(lbm_kernel<R, S, DEV, true, int>);
             else launch(lbm_kernel<R, S, DEV, false, int>);
