@@ -71,8 +71,11 @@ __global__ void __launch_bounds__(TL::NT) ens_fused_kernel(const EnsBox* __restr
     }
 }
 
+// Held to the single-box walled LBM kernel's register budget (5 blocks per SM
+// for FP32 compute, 2 for FP64); each work item's box picks the periodic or the
+// walled gather (block-uniform).
 template <class R, class S, bool DEV>
-__global__ void __launch_bounds__(256) ens_lbm_kernel(const EnsBox* __restrict__ boxes,
+__global__ void __launch_bounds__(256, lbm_min_blocks<R, S, true>()) ens_lbm_kernel(const EnsBox* __restrict__ boxes,
                                                       const EnsLbmWork* __restrict__ work, int nwork, int par,
                                                       int first, int write_rho_all) {
     for (int w = blockIdx.x; w < nwork; w += gridDim.x) {
@@ -92,7 +95,10 @@ __global__ void __launch_bounds__(256) ens_lbm_kernel(const EnsBox* __restrict__
         R* rho_buf = (R*)B.rho;
         const R* F = (const R*)B.F;
         R f[15];
-        load_pre<R, S>(P, K, first != 0, (const S*)B.f[par], c, q, (mv && !first) ? rho_buf[c] : R(0), f);
+        if (P.uper[0] && P.uper[2] && P.uper[4])
+            load_pre<R, S, false>(P, K, first != 0, (const S*)B.f[par], c, q, R(0), f);
+        else
+            load_pre<R, S, true>(P, K, first != 0, (const S*)B.f[par], c, q, (mv && !first) ? rho_buf[c] : R(0), f);
         R rho, ux, uy, uz;
         collide<R, DEV>(K, f, F[c], F[V + c], F[2 * V + c], rho, ux, uy, uz);
         S* fout = (S*)B.f[1 - par];
