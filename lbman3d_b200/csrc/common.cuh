@@ -45,6 +45,8 @@ struct SimParams {
     Phys<float> pf;        // read them in place from the parameter space
 };
 
+static_assert(sizeof(SimParams) % 4 == 0, "copied to shared memory as 32-bit words");
+
 // Constants of precision R, referenced inside the kernel's (grid-constant)
 // parameter struct, so dynamic indexing needs no local copy.
 template <class R>

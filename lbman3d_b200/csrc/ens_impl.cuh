@@ -56,9 +56,12 @@ struct EnsImpl {
             const int x = xy[0], y = xy[1];
             impl::with_tile<R>(x, y, [&](auto tl) {
                 using TL = decltype(tl);
+                // the tile's own staging (the Q kernel may also hold static
+                // shared memory, so the device maximum would not fit)
+                const size_t need = std::min(max_smem, TL::template smem_bytes<R>());
                 auto attr = [&](auto kern) {
                     if (e == cudaSuccess)
-                        e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)max_smem);
+                        e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)need);
                 };
                 attr(ens_qforce_kernel<TL, R, true>);
                 attr(ens_qforce_kernel<TL, R, false>);
