@@ -170,13 +170,16 @@ int lbman_reduce(lbman_solver* s, int flags, lbman_diag* out);
  *
  * Scratch comes from a fixed array inside the library (partial sums of at
  * most LBMAN_NOALLOC_MAX_BLOCKS blocks, about 76 KB per device, held by every
- * GPU that loads the library until the process exits).  The first call on a
- * device looks up that array's device address; make that first call before
- * any stream capture.  All calls share the array: calls whose GPU work
- * overlaps (other streams or threads, same device) race and corrupt each
- * other's results; serialise them.  ncells above LBMAN_NOALLOC_MAX_CELLS is
- * rejected with LBMAN_ERR_ARG.  Allocates nothing: no cudaMalloc, no
- * cudaFree, no allocating library call.                                     */
+ * GPU that loads the library until the process exits).  Each call looks up
+ * that array's device address in the current device's context.  The call
+ * copies its result to the host and synchronises cuda_stream, so it cannot be
+ * issued while that stream is being captured.  All calls share the array:
+ * calls whose GPU work overlaps (other streams or threads, same device) race
+ * and corrupt each other's results; serialise them.  A CUDA error already
+ * pending on the calling thread is reported (LBMAN_ERR_CUDA) and left
+ * pending.  ncells above LBMAN_NOALLOC_MAX_CELLS is rejected with
+ * LBMAN_ERR_ARG.  Allocates nothing: no cudaMalloc, no cudaFree, no
+ * allocating library call.                                                  */
 #define LBMAN_NOALLOC_MAX_BLOCKS 1184
 #define LBMAN_NOALLOC_MAX_CELLS 2147483647LL
 int lbman_flow_reduce_noalloc(int64_t ncells, int precision, const void* rho, const void* u3,

@@ -42,29 +42,24 @@ __global__ void __launch_bounds__(TL::NT, (Stage<TL, R>::MINB)) ens_qforce_kerne
     extern __shared__ __align__(16) unsigned char smem_raw[];
     // The item's box parameters, copied to shared memory once per item: the
     // z march reads them throughout, and a global-memory copy would cost a
-    // load per use where a single-box launch reads its constant bank.
-    // (Only where the tile's staging leaves room within one block's 227 KB.)
-    constexpr bool kCopy = Stage<TL, R>::bytes + sizeof(SimParams) + 1024 <= 227 * 1024;
+    // load per use where a single-box launch reads its constant bank.  Every
+    // tile whose staging fits one block (227 KB) leaves room for the copy
+    // (largest: FP64 32x8, 216 672 B staging + 1 368 B of parameters).
+    static_assert(Stage<TL, R>::bytes + sizeof(SimParams) + 1024 <= 227 * 1024,
+                  "the box parameters must fit beside the tile's staging");
     for (int w = blockIdx.x; w < nwork; w += gridDim.x) {
         const EnsQWork it = work[w];
         const EnsBox& B = boxes[it.box];
         const int z0 = it.bz * B.zc;
-        if constexpr (kCopy) {
-            __shared__ __align__(16) uint32_t pbuf[sizeof(SimParams) / 4];
-            const SimParams& Ps = *reinterpret_cast<const SimParams*>(pbuf);
-            const uint32_t* src = reinterpret_cast<const uint32_t*>(&B.P);
-            for (int i = threadIdx.x; i < (int)(sizeof(SimParams) / 4); i += blockDim.x) pbuf[i] = src[i];
-            __syncthreads();
-            if (z0 < Ps.nz)
-                qf_march<TL, R, UPWIND>(Ps, it.bx * TL::TCX, it.by * TL::TCY, z0, min(z0 + B.zc, Ps.nz),
-                                        (const R*)B.q[par], (const R*)B.u[0], reinterpret_cast<R*>(smem_raw),
-                                        StoreQForce<R>{(R*)B.q[1 - par], (R*)B.F, Ps.V});
-        } else {
-            if (z0 < B.P.nz)
-                qf_march<TL, R, UPWIND>(B.P, it.bx * TL::TCX, it.by * TL::TCY, z0, min(z0 + B.zc, B.P.nz),
-                                        (const R*)B.q[par], (const R*)B.u[0], reinterpret_cast<R*>(smem_raw),
-                                        StoreQForce<R>{(R*)B.q[1 - par], (R*)B.F, B.P.V});
-        }
+        __shared__ __align__(16) uint32_t pbuf[sizeof(SimParams) / 4];
+        const SimParams& Ps = *reinterpret_cast<const SimParams*>(pbuf);
+        const uint32_t* src = reinterpret_cast<const uint32_t*>(&B.P);
+        for (int i = threadIdx.x; i < (int)(sizeof(SimParams) / 4); i += blockDim.x) pbuf[i] = src[i];
+        __syncthreads();
+        if (z0 < Ps.nz)
+            qf_march<TL, R, UPWIND>(Ps, it.bx * TL::TCX, it.by * TL::TCY, z0, min(z0 + B.zc, Ps.nz),
+                                    (const R*)B.q[par], (const R*)B.u[0], reinterpret_cast<R*>(smem_raw),
+                                    StoreQForce<R>{(R*)B.q[1 - par], (R*)B.F, Ps.V});
         __syncthreads();  // the staging rings and the parameters are reused by the next item
     }
 }

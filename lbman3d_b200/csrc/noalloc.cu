@@ -13,15 +13,17 @@
 // The scratch is g_partials below: one FP64 partial sum per reduction block
 // and quantity, plus g_result for the folded totals.  It is a __device__
 // array, so every GPU that loads the library holds it (about 76 KB) until the
-// process exits.  Host code cannot use the symbol's name as a device address;
-// the address is fetched once per device with cudaGetSymbolAddress while that
-// device is current (on the first call made on it) and passed to the kernels.
+// process exits.  Host code cannot use the symbol's name as a device address:
+// every call fetches the address with cudaGetSymbolAddress while the caller's
+// device is current and passes it to the kernels.  The lookup is a table
+// search inside the CUDA runtime (no allocation), and doing it per call keeps
+// the address right when the device's context was torn down and re-created
+// (cudaDeviceReset reloads the module, and the array can move).
 #include <cuda_runtime.h>
 
 #include <cmath>
 #include <cstdio>
 #include <cstring>
-#include <mutex>
 
 #include "../../include/lbman3d.h"
 #include "reduce.cuh"
@@ -35,41 +37,20 @@ namespace {
 using namespace lbman;
 
 constexpr int kMaxBlocks = LBMAN_NOALLOC_MAX_BLOCKS;
-constexpr int kMaxDevices = 64;
 
 static __device__ __align__(256) double g_partials[kMaxBlocks * kFlowQ];
 static __device__ __align__(256) double g_result[16];
-
-struct DeviceScratch {
-    double* partials = nullptr;
-    double* result = nullptr;
-    bool ready = false;
-};
-DeviceScratch g_dev[kMaxDevices];
-std::mutex g_mu;
 
 int fail(int code, const char* msg) {
     lbman::set_last_error(msg);  // reported by lbman_last_error()
     return code;
 }
 
-// Device addresses of the scratch arrays for the current device.
-int scratch_for_current_device(DeviceScratch** out) {
-    int dev = 0;
-    if (cudaGetDevice(&dev) != cudaSuccess) return fail(LBMAN_ERR_CUDA, "cudaGetDevice failed");
-    if (dev < 0 || dev >= kMaxDevices) return fail(LBMAN_ERR_UNSUPPORTED, "device ordinal out of range");
-    std::lock_guard<std::mutex> lock(g_mu);
-    DeviceScratch& d = g_dev[dev];
-    if (!d.ready) {
-        cudaError_t e1 = cudaGetSymbolAddress((void**)&d.partials, g_partials);
-        cudaError_t e2 = cudaGetSymbolAddress((void**)&d.result, g_result);
-        if (e1 != cudaSuccess || e2 != cudaSuccess) {
-            d.partials = d.result = nullptr;
-            return fail(LBMAN_ERR_CUDA, "cudaGetSymbolAddress of the reduction scratch failed");
-        }
-        d.ready = true;
-    }
-    *out = &d;
+// Device addresses of the scratch arrays in the current device's context.
+int scratch_for_current_device(double** partials, double** result) {
+    if (cudaGetSymbolAddress((void**)partials, g_partials) != cudaSuccess ||
+        cudaGetSymbolAddress((void**)result, g_result) != cudaSuccess)
+        return fail(LBMAN_ERR_CUDA, "cudaGetSymbolAddress of the reduction scratch failed");
     return LBMAN_OK;
 }
 
@@ -82,8 +63,14 @@ extern "C" int lbman_flow_reduce_noalloc(int64_t ncells, int precision, const vo
         return fail(LBMAN_ERR_ARG, "ncells must be in [1, LBMAN_NOALLOC_MAX_CELLS]");
     if (precision != LBMAN_FP64 && precision != LBMAN_FP32)
         return fail(LBMAN_ERR_ARG, "precision must be LBMAN_FP64 (double fields) or LBMAN_FP32 (float fields)");
-    DeviceScratch* d = nullptr;
-    if (int st = scratch_for_current_device(&d)) return st;
+    // An error left pending by earlier, unrelated work is the caller's to
+    // see: report it without clearing it, so the launch checks below see only
+    // this call's launches.
+    if (cudaPeekAtLastError() != cudaSuccess)
+        return fail(LBMAN_ERR_CUDA, "a CUDA error was already pending before the call");
+    double* partials = nullptr;
+    double* result = nullptr;
+    if (int st = scratch_for_current_device(&partials, &result)) return st;
 
     SimParams P;
     std::memset(&P, 0, sizeof(P));
@@ -94,16 +81,17 @@ extern "C" int lbman_flow_reduce_noalloc(int64_t ncells, int precision, const vo
     cudaStream_t st = (cudaStream_t)cuda_stream;
     if (precision == LBMAN_FP64)
         flow_reduce_kernel<double><<<G, kRedThreads, 0, st>>>(P, (const double*)rho, (const double*)u3,
-                                                               (double*)upast3, d->partials);
+                                                               (double*)upast3, partials);
     else
         flow_reduce_kernel<float><<<G, kRedThreads, 0, st>>>(P, (const float*)rho, (const float*)u3,
-                                                             (float*)upast3, d->partials);
+                                                             (float*)upast3, partials);
+    if (cudaGetLastError() != cudaSuccess) return fail(LBMAN_ERR_CUDA, "flow reduction launch failed");
     // Every partial the fold reads, and every result slot copied back, is
     // written earlier in this call, so nothing has to be cleared first.
-    fold_partials_kernel<<<1, 1024, 0, st>>>(d->partials, G, kFlowQ, 1, d->result);
-    if (cudaGetLastError() != cudaSuccess) return fail(LBMAN_ERR_CUDA, "reduction launch failed");
+    fold_partials_kernel<<<1, 1024, 0, st>>>(partials, G, kFlowQ, 1, result);
+    if (cudaGetLastError() != cudaSuccess) return fail(LBMAN_ERR_CUDA, "fold launch failed");
     double r[kFlowQ];
-    if (cudaMemcpyAsync(r, d->result, sizeof(r), cudaMemcpyDeviceToHost, st) != cudaSuccess ||
+    if (cudaMemcpyAsync(r, result, sizeof(r), cudaMemcpyDeviceToHost, st) != cudaSuccess ||
         cudaStreamSynchronize(st) != cudaSuccess)
         return fail(LBMAN_ERR_CUDA, "copy of the reduction result failed");
     std::memset(out, 0, sizeof(*out));

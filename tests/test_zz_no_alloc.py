@@ -31,11 +31,20 @@ def _noalloc(ncells, precision, rho, u, upast, stream):
     return {k: getattr(d, k) for k in KEYS} | {"nan_detected": d.nan_detected, "defect_faces": d.defect_faces}
 
 
+# 40x36x28 = 40 320 cells needs 158 reduction blocks of 256 threads; 96^3 =
+# 884 736 cells is above 1184 x 256, so the grid is capped at the scratch
+# array's 1184 blocks, each thread sums several cells and the fold runs over
+# the whole array.
+GRIDS = {"small": (40, 36, 28), "capped": (96, 96, 96)}
+
+
+@pytest.mark.parametrize("grid", list(GRIDS), ids=list(GRIDS))
 @pytest.mark.parametrize("precision", [L.Precision.FP64, L.Precision.FP32], ids=["fp64", "fp32"])
-def test_noalloc_flow_reduce_matches_lbman_reduce_on_two_calls(precision):
+def test_noalloc_flow_reduce_matches_lbman_reduce_on_two_calls(precision, grid):
     import torch
 
-    p = L.Params(nx=40, ny=36, nz=28, ALPHA=0.01)
+    nx, ny, nz = GRIDS[grid]
+    p = L.Params(nx=nx, ny=ny, nz=nz, ALPHA=0.01)
     V = p.V
     dtype = torch.float64 if precision == L.Precision.FP64 else torch.float32
     sim = L.Simulation(p, L.ChannelConfig(), precision)
