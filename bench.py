@@ -1,13 +1,14 @@
-"""Benchmark of the fused sm_100a time step (contract: one JSON line on rank 0).
+"""Benchmark of the sm_100a time step (contract: one JSON line on rank 0).
 
-Default workload: SlitConfig (free-slip plates confining x) 64x256x256,
-params.h defaults with zeta (ALPHA) = 0.01, centred advection, FP32 compute
-with populations stored as FP32 deviations, seeded random-director initial
-condition.  A "step" is one full time step (Q-tensor update + body force +
-D3Q15 collide/stream) over the whole box.
+Default workload: FullyPeriodicConfig 512x512x512, params.h defaults with
+zeta (ALPHA) = 0.01 and LAMBDA = 0.3, centred advection, FP32 compute with
+populations stored as FP32 deviations, seeded random-director initial
+condition (the precision configuration, the largest single-GPU one).  A
+"step" is one full time step (Q-tensor update + body force + D3Q15
+collide/stream) over the whole box.
 
     python bench.py [--gpus N] [--steps K] [--warmup W] [--impl reference]
-                    [--workload slit64|channel20|periodic512|periodic32]
+                    [--workload periodic512|slit64|channel20|periodic32]
                     [--precision fp32|fp64|fp16]
 
 value    : MLUPS (million lattice-cell updates per second), all GPUs, device
@@ -16,9 +17,12 @@ value    : MLUPS (million lattice-cell updates per second), all GPUs, device
 e2e      : the same metric through the C ABI with host (pinned) buffers: each
            e2e step uploads rho/u/Q, runs kSaveInterval = 100 solver steps and
            downloads rho/u/Q, as ActiveNematicSim's save cycle does.
-roofline : algorithmic bytes per cell update (f 15+15, Q 5+5, u 3+3 words;
-           184 B in FP32) x cells / average fused-kernel duration, against the
-           measured HBM copy bandwidth.
+roofline : algorithmic bytes per cell update of the dominant kernel (Q+force:
+           Q, u read, Q_new, F written; LBM: f*, F read, f*, u written) x cells
+           / its average duration, against the measured HBM copy bandwidth;
+           the whole step against 184 B/cell (f 15+15, Q 5+5, u 3+3 words).
+error_vs_fp64 : FP32 and FP16-storage fields against the FP64 path (bitwise
+           the reference's arithmetic) from the same seed after 2000 steps.
 --impl reference : the reference's own OpenMP CPU solver (oracle/_ref build
            of its sources) on this machine's host cores, bounded sample.
 """
@@ -40,11 +44,16 @@ sys.path.insert(0, ROOT)
 
 WORKLOADS = {
     # name: (nx, ny, nz, bc, ALPHA, ref_build)
+    "periodic512": (512, 512, 512, "periodic", 0.01, "b_p512"),
     "slit64": (64, 256, 256, "slit", 0.01, "b_slit"),
     "channel20": (20, 100, 100, "channel", 0.01, "b_channel"),
-    "periodic512": (512, 512, 512, "periodic", 0.01, None),
     "periodic32": (32, 32, 32, "periodic", 0.023, "b_p32"),
 }
+SEED, S0, SIGMA = 1234, 0.5, 1e-3
+# Host bytes per cell of the reference's CPU solver: FluidFields (f, f_new,
+# force, rho, u: 37 doubles) + QTensorFields (Q, Q_new, Sigma, tau: 18) and the
+# seeded field while it is injected (5).
+REF_HOST_BYTES_PER_CELL = 8 * (37 + 18 + 5)
 BYTES_PER_CELL = {"fp64": 368, "fp32": 184, "fp16": 124}
 
 
@@ -134,8 +143,7 @@ def make_sim(workload, precision, device, kernels="auto", tile=None):
 def time_device(sim, steps, warmup, stream):
     """Device-resident steps timed with CUDA events on the solver's stream."""
     import torch
-    S0 = 0.5
-    sim.init_seeded(1234, S0, 1e-3)
+    sim.init_seeded(SEED, S0, SIGMA)
     sim.step(warmup)
     sim.synchronize()
     l0 = sim.launch_count()
@@ -225,22 +233,58 @@ def ensemble_vs_sequential(device, stream, nboxes=96, steps=200, seq_steps=40):
             "shape": {k: tuned[k] for k in ("kernels", "tile_x", "tile_y", "zchunk")}}
 
 
-def error_vs_fp64(workload, precision, device, nsteps=100):
-    """Per-field max relative error against the FP64 path (bitwise the
-    reference arithmetic) on the same seed after nsteps."""
-    a, _ = make_sim(workload, precision, device)
-    b, _ = make_sim(workload, "fp64", device)
-    for s in (a, b):
-        s.init_seeded(1234, 0.5, 1e-3)
+def max_rel_err(a, b, chunk=1 << 24):
+    """max|a - b| / max|b| over one field, in chunks (bounded temporaries)."""
+    num = den = 0.0
+    for i in range(0, a.size, chunk):
+        x, y = a[i:i + chunk], b[i:i + chunk]
+        num = max(num, float(np.max(np.abs(x - y))))
+        den = max(den, float(np.max(np.abs(y))))
+    return num / max(den, 1e-300)
+
+
+def errors_vs_fp64(workload, precisions, device, nsteps):
+    """Per-field max relative error of each precision against the FP64 path
+    (bitwise the reference arithmetic) on the same seed after nsteps; one FP64
+    run serves every precision.  Device time of each run is reported too."""
+    import torch
+
+    def run(prec):
+        s, _ = make_sim(workload, prec, device)
+        s.init_seeded(SEED, S0, SIGMA)
+        s.synchronize()
+        t0 = time.perf_counter()
         s.step(nsteps)
-    x, y = a.download(), b.download()
-    a.close(), b.close()
-    out = {}
-    for f in ("rho", "u", "q"):  # max|a - b| / max|b|, per field
-        out[f] = float(np.max(np.abs(x[f] - y[f])) / max(np.max(np.abs(y[f])), 1e-300))
-    out["steps"] = nsteps
-    out["metric"] = "max|a-b|/max|b| against the FP64 path (bitwise the reference arithmetic), same seed"
-    return out
+        s.synchronize()
+        dt = time.perf_counter() - t0
+        out = s.download()
+        s.close()
+        torch.cuda.empty_cache()
+        return out, dt
+
+    ref, t_ref = run("fp64")
+    res = {"steps": nsteps, "fp64_run_s": t_ref,
+           "metric": "max|a-b|/max|b| per field against the FP64 path (bitwise the reference arithmetic), "
+                     "same seed, same steps"}
+    for prec in precisions:
+        x, dt = run(prec)
+        res[prec] = {f: max_rel_err(x[f], ref[f]) for f in ("rho", "u", "q")}
+        res[prec]["run_s"] = dt
+        res[prec]["nan"] = bool(not all(np.isfinite(x[f]).all() for f in ("rho", "u", "q")))
+        del x
+    return res
+
+
+def host_mem_available():
+    """MemAvailable of this host in bytes (None where /proc/meminfo is absent)."""
+    try:
+        with open("/proc/meminfo") as fh:
+            for line in fh:
+                if line.startswith("MemAvailable:"):
+                    return int(line.split()[1]) * 1024
+    except OSError:
+        pass
+    return None
 
 
 def reduce_max(value, world, device):
@@ -266,12 +310,11 @@ def time_e2e(sim, p, iters, stream, save_interval=100, world=1, device=None):
     V = p.V
     pin = lambda n: torch.empty(n, dtype=torch.float64, pin_memory=True).numpy()
     rho, u, q = pin(V), pin(3 * V), pin(5 * V)
-    sim.init_seeded(99, 0.5, 1e-3)
-    out = sim.download()
-    rho[:], u[:], q[:] = out["rho"], out["u"], out["q"]
     orho, ou, oq = pin(V), pin(3 * V), pin(5 * V)
     from lbman3d_b200 import _native as N
     lib, h = N.lib(), sim.handle
+    sim.init_seeded(99, S0, SIGMA)
+    N.check(lib.lbman_download(h, N.dptr(rho), N.dptr(u), N.dptr(q), None, None))
 
     def cycle():
         N.check(lib.lbman_upload(h, N.dptr(rho), N.dptr(u), N.dptr(q), None, None))
@@ -293,50 +336,81 @@ def time_e2e(sim, p, iters, stream, save_interval=100, world=1, device=None):
 
 
 def reference_cpu(workload, max_steps, warmup):
-    """The reference's OpenMP CPU solver on the host cores (oracle/_ref)."""
+    """The reference's OpenMP CPU solver on the host cores (oracle/_ref build
+    of its own sources), on the seeded initial condition of the workload,
+    generated inside the driver.  Raises RuntimeError when the host cannot
+    hold the reference's fields."""
     from oracle import build_ref
-    from oracle import oracle as O
     nx, ny, nz, bc, alpha, tag = WORKLOADS[workload]
     exe = build_ref.driver_path(tag) if tag else None
     cores = os.cpu_count() or 1
     V = nx * ny * nz
-    sys.path.insert(0, os.path.join(ROOT, "tests", "golden"))
-    from cases import BC
-    op = O.make_params(nx, ny, nz, BC[bc], ALPHA=alpha)
-    q = O.seeded_q(op, 1234, O.equilibrium_order(op), 1e-3)
+    need = REF_HOST_BYTES_PER_CELL * V
+    avail = host_mem_available()
+    if avail is not None and need > 0.9 * avail:
+        raise RuntimeError(f"the reference CPU solver needs {need / 1e9:.0f} GB of host memory for "
+                           f"{nx}x{ny}x{nz}; {avail / 1e9:.0f} GB available")
     if exe and os.path.exists(exe):
-        with tempfile.TemporaryDirectory() as td:
-            fin = os.path.join(td, "in.bin")
-            with open(fin, "wb") as fh:
-                fh.write(np.int64(V).tobytes() + np.int32(0).tobytes() + np.int32(0).tobytes())
-                fh.write(np.ones(V).tobytes() + np.zeros(3 * V).tobytes() + q.tobytes())
-            r = subprocess.run([exe, "--bench", bc, fin, str(warmup), str(max_steps)], capture_output=True,
-                               text=True, env=dict(os.environ, LBMAN_REF_THREADS=str(cores), OMP_NUM_THREADS=str(cores)),
-                               check=True)
-            d = json.loads(r.stdout.strip().splitlines()[-1])
+        r = subprocess.run([exe, "--bench", bc, str(SEED), repr(S0), repr(SIGMA), str(warmup), str(max_steps)],
+                           capture_output=True, text=True,
+                           env=dict(os.environ, LBMAN_REF_THREADS=str(cores), OMP_NUM_THREADS=str(cores)),
+                           check=True)
+        d = json.loads(r.stdout.strip().splitlines()[-1])
         return {"value": d["mlups"], "unit": "MLUPS", "cores": d["threads"], "kind": "reference",
                 "sample": f"{max_steps} full time steps of the {nx}x{ny}x{nz} box after {warmup} warm-up "
                           f"(reference CPU solver built from its sources, OpenMP)", "ms_step": d["ms_step"]}
-    # C restatement (single thread per call site of OpenMP in the port)
+    # C restatement (one thread)
+    from oracle import oracle as O
+    sys.path.insert(0, os.path.join(ROOT, "tests", "golden"))
+    from cases import BC
+    op = O.make_params(nx, ny, nz, BC[bc], ALPHA=alpha)
+    q = O.seeded_q(op, SEED, O.equilibrium_order(op), SIGMA)
     sim = O.OracleSim(op)
     sim.set(np.ones(V), np.zeros(3 * V), q)
     sim.step(warmup)
     t0 = time.perf_counter()
     sim.step(max_steps)
     dt = time.perf_counter() - t0
-    return {"value": V * max_steps / dt / 1e6, "unit": "MLUPS", "cores": cores, "kind": "port",
+    return {"value": V * max_steps / dt / 1e6, "unit": "MLUPS", "cores": 1, "kind": "port",
             "sample": f"{max_steps} full time steps of the {nx}x{ny}x{nz} box (C restatement)",
             "ms_step": dt * 1e3 / max_steps}
+
+
+def ref_sample_steps(V, steps):
+    """Steps of a bounded CPU sample: about half a minute of reference work."""
+    return max(1, min(steps, 3 if V > 5e7 else 20 if V > 1e6 else 200))
+
+
+def side_workloads(names, device, stream, steps=2000):
+    """The other single-GPU solver workloads (channel and slit configurations),
+    FP32, autotuned, device-timed: MLUPS and the whole step's HBM fraction."""
+    peak, _ = measured_peaks()
+    out = {}
+    for w in names:
+        nx, ny, nz, bc, alpha, _ = WORKLOADS[w]
+        s, p = make_sim(w, "fp32", device)
+        s.set_stream(stream.cuda_stream)
+        s.init_seeded(SEED, S0, SIGMA)
+        tuned = s.autotune(steps_per_trial=10)
+        ms, _ = time_device(s, steps, 20, stream)
+        s.close()
+        out[f"{bc}_{nx}x{ny}x{nz}"] = {"value": p.V * steps / (ms * 1e3), "unit": "MLUPS", "steps": steps,
+                                       "ms_per_step": ms / steps,
+                                       "step_frac": BYTES_PER_CELL["fp32"] * p.V / (ms / steps * 1e-3) / 1e9 / peak,
+                                       "shape": {k: tuned[k] for k in ("kernels", "tile_x", "tile_y", "zchunk")}}
+    return out
 
 
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
-    ap.add_argument("--steps", type=int, default=10000)
-    ap.add_argument("--warmup", type=int, default=50)
+    ap.add_argument("--steps", type=int, default=200)
+    ap.add_argument("--warmup", type=int, default=10)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
-    ap.add_argument("--workload", default="slit64", choices=list(WORKLOADS))
+    ap.add_argument("--workload", default="periodic512", choices=list(WORKLOADS))
     ap.add_argument("--precision", default="fp32", choices=["fp32", "fp64", "fp16"])
+    ap.add_argument("--error-steps", type=int, default=2000,
+                    help="steps of the FP32/FP16 runs compared with the FP64 path")
     ap.add_argument("--no-extras", action="store_true", help="skip e2e, cpu baseline and variants")
     ap.add_argument("--kernels", default="auto", choices=["auto", "fused", "split"])
     ap.add_argument("--tile", default=None, help="tcx,tcy[,zchunk] of the z-marching kernels")
@@ -346,17 +420,22 @@ def main():
     world = int(os.environ.get("WORLD_SIZE", "1"))
     nx, ny, nz, bc, alpha, _ = WORKLOADS[a.workload]
     V = nx * ny * nz
-    config = {"workload": f"{bc}_{nx}x{ny}x{nz}", "bc": bc, "zeta": alpha, "advection": "centred",
-              "init": "seeded random director, S0=0.5, 1e-3 Gaussian", "l2": "state larger than L2 (126 MB)"
-              if V * BYTES_PER_CELL[a.precision] > 126e6 else "state fits in L2", "parallelism": f"replicas x{a.gpus}"}
+    config = {"workload": f"{bc}_{nx}x{ny}x{nz}", "bc": bc, "zeta": alpha, "LAMBDA": 0.3, "advection": "centred",
+              "init": f"seeded random director (seed {SEED}), S0={S0}, {SIGMA:g} Gaussian",
+              "l2": "state larger than L2 (126 MB)" if V * BYTES_PER_CELL[a.precision] > 126e6
+              else "state fits in L2", "parallelism": f"replicas x{a.gpus}"}
 
     if a.impl == "reference":
         if rank != 0:
             return
-        n = max(1, min(a.steps, 20 if V > 1e6 else 200))
-        r = reference_cpu(a.workload, n, min(a.warmup, 2))
+        n, w = ref_sample_steps(V, a.steps), min(a.warmup, 1)
+        try:
+            r = reference_cpu(a.workload, n, w)
+        except (RuntimeError, subprocess.CalledProcessError, OSError) as e:
+            print(json.dumps({"impl": "reference", "unavailable": str(e)[:300]}), flush=True)
+            return
         line = {"impl": "reference", "metric": "MLUPS", "value": r["value"], "unit": "MLUPS", "n_gpus": a.gpus,
-                "steps": n, "warmup": min(a.warmup, 2), "ms_per_step": r["ms_step"], "higher_is_better": True,
+                "steps": n, "warmup": w, "ms_per_step": r["ms_step"], "higher_is_better": True,
                 "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic", "config": config,
                 "cpu_baseline": {k: r[k] for k in ("value", "unit", "cores", "kind", "sample")},
                 "e2e": {"value": r["value"], "unit": "MLUPS", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
@@ -376,7 +455,7 @@ def main():
     sim, p = make_sim(a.workload, a.precision, local, a.kernels, tile)
     sim.set_stream(stream.cuda_stream)
     if a.kernels == "auto" and not tile:
-        sim.init_seeded(1234, 0.5, 1e-3)
+        sim.init_seeded(SEED, S0, SIGMA)
         tuned = sim.autotune(steps_per_trial=8 if V > 5e7 else 10)
         config["autotuned"] = {k: tuned[k] for k in ("kernels", "tile_x", "tile_y", "zchunk", "trials")}
     sh = sim.shape()
@@ -396,6 +475,8 @@ def main():
     kern = kernel_breakdown(sim, config["kernels"], a.precision, V, stream, 30 if V > 5e7 else 200)
     dom = max(kern, key=lambda k: kern[k]["ms"])
     achieved = kern[dom]["bytes_per_cell"] * V / (kern[dom]["ms"] * 1e-3) / 1e9
+    for k in kern:
+        kern[k]["frac"] = kern[k]["bytes_per_cell"] * V / (kern[k]["ms"] * 1e-3) / 1e9 / peak
     line = {"metric": "MLUPS", "value": mlups, "unit": "MLUPS", "n_gpus": world, "steps": a.steps,
             "warmup": max(a.warmup, 3), "ms_per_step": ms_step, "higher_is_better": True, "scaling": "weak",
             "vs_baseline": None, "dtype": {"fp32": "f32", "fp64": "f64", "fp16": "f32 (f16 storage)"}[a.precision],
@@ -408,30 +489,34 @@ def main():
             "clocks": clk.summary()}
     if not a.no_extras:
         line["e2e"] = time_e2e(sim, p, 5, stream, world=world, device="cuda")
-        if world == 1:  # single-GPU extras; at N > 1 every rank runs only the legs above
-            line["error_vs_fp64"] = error_vs_fp64(a.workload, a.precision, local) if a.precision != "fp64" else None
-            variants = {}
-            for prec in ("fp64", "fp16"):
-                if prec == a.precision:
-                    continue
-                s2, _ = make_sim(a.workload, prec, local)
-                s2.set_stream(stream.cuda_stream)
-                s2.init_seeded(1234, 0.5, 1e-3)
-                tuned2 = s2.autotune(steps_per_trial=3)
-                n2 = max(200, a.steps // 5)
-                ms2, _ = time_device(s2, n2, 10, stream)
-                variants[prec] = {"value": V * n2 / (ms2 * 1e3), "unit": "MLUPS", "steps": n2,
-                                  "frac": BYTES_PER_CELL[prec] * V / (ms2 / n2 * 1e-3) / 1e9 / peak,
-                                  "shape": {k: tuned2[k] for k in ("kernels", "tile_x", "tile_y", "zchunk")}}
-                s2.close()
-            line["variants"] = variants
-            line["ensemble"] = ensemble_vs_sequential(local, stream)
-            try:
-                line["cpu_baseline"] = {k: v for k, v in reference_cpu(a.workload, 5 if V > 1e6 else 50, 1).items()
-                                        if k != "ms_step"}
-            except Exception as e:  # the baseline is reported, never required
-                line["cpu_baseline"] = {"value": None, "unit": "MLUPS", "error": str(e)[:200]}
     sim.close()
+    torch.cuda.empty_cache()
+    if not a.no_extras and world == 1:  # single-GPU extras; at N > 1 every rank runs only the legs above
+        line["error_vs_fp64"] = errors_vs_fp64(a.workload, ["fp32", "fp16"], local, a.error_steps)
+        variants = {}
+        for prec in ("fp64", "fp16", "fp32"):
+            if prec == a.precision:
+                continue
+            s2, _ = make_sim(a.workload, prec, local)
+            s2.set_stream(stream.cuda_stream)
+            s2.init_seeded(SEED, S0, SIGMA)
+            tuned2 = s2.autotune(steps_per_trial=3)
+            n2 = max(100, a.steps // 2)
+            ms2, _ = time_device(s2, n2, 10, stream)
+            variants[prec] = {"value": V * n2 / (ms2 * 1e3), "unit": "MLUPS", "steps": n2,
+                              "frac": BYTES_PER_CELL[prec] * V / (ms2 / n2 * 1e-3) / 1e9 / peak,
+                              "shape": {k: tuned2[k] for k in ("kernels", "tile_x", "tile_y", "zchunk")}}
+            s2.close()
+            torch.cuda.empty_cache()
+        line["variants"] = variants
+        line["other_workloads"] = side_workloads([w for w in ("slit64", "channel20") if w != a.workload], local,
+                                                 stream)
+        line["ensemble"] = ensemble_vs_sequential(local, stream)
+        try:
+            r = reference_cpu(a.workload, ref_sample_steps(V, a.steps), 1)
+            line["cpu_baseline"] = {k: v for k, v in r.items() if k != "ms_step"}
+        except Exception as e:  # the baseline is reported, never required
+            line["cpu_baseline"] = {"value": None, "unit": "MLUPS", "error": str(e)[:300]}
     if rank == 0:
         print(json.dumps(line), flush=True)
     if world > 1:

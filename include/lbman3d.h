@@ -326,6 +326,15 @@ int lbman_closure_train(lbman_closure* c, int iters, float lr, uint64_t seed, do
  * during lbman_closure_train (0 = none, the default); gain: multiplier of the
  * correction in lbman_closure_step (1 = default).                          */
 int lbman_closure_set_options(lbman_closure* c, float train_noise, float gain);
+/* Polls of each tensor-core completion wait of the closure's kernels before
+ * the wait gives up (default LBMAN_CLOSURE_WAIT_DEFAULT).  A wait that gives
+ * up makes the call return LBMAN_ERR_TIMEOUT; the kernel still lets every
+ * MMA it issued finish (that drain keeps the default limit) before it frees
+ * its tensor memory, so the next call runs normally.  0 makes the first
+ * completion wait of every CTA give up: a way to exercise the timeout path.
+ * No counterpart in the reference.                                          */
+#define LBMAN_CLOSURE_WAIT_DEFAULT 67108864u
+int lbman_closure_set_wait_limit(lbman_closure* c, uint32_t polls);
 /* Coarse solver state := snapshot k.                                        */
 int lbman_closure_load_snapshot(lbman_closure* c, int k, lbman_solver* coarse);
 /* nsteps corrected coarse steps: network on the current state, populations

@@ -57,6 +57,7 @@ class lbman_stats(C.Structure):
 
 
 STATS_MAX_BINS = 8192
+CLOSURE_WAIT_DEFAULT = 67108864  # LBMAN_CLOSURE_WAIT_DEFAULT
 
 
 class LbmanError(RuntimeError):
@@ -136,6 +137,7 @@ PROTOTYPES = [
     ("lbman_closure_load_snapshot", C.c_int, [C.c_void_p, C.c_int, C.c_void_p]),
     ("lbman_closure_step", C.c_int, [C.c_void_p, C.c_void_p, C.c_int]),
     ("lbman_closure_set_options", C.c_int, [C.c_void_p, C.c_float, C.c_float]),
+    ("lbman_closure_set_wait_limit", C.c_int, [C.c_void_p, C.c_uint32]),
     ("lbman_flow_reduce_noalloc", C.c_int,
      [C.c_int64, C.c_int, C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p, C.POINTER(lbman_diag)]),
 ]

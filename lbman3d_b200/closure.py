@@ -123,5 +123,12 @@ class Closure:
         """Input noise (std, normalised units) in training; correction gain."""
         N.check(N.lib().lbman_closure_set_options(self._h, float(train_noise), float(gain)))
 
+    def set_wait_limit(self, polls: int = None):
+        """Polls of each tensor-core completion wait before it gives up
+        (None: the default); a wait that gives up makes the call raise with
+        status LBMAN_ERR_TIMEOUT, and the next call runs normally."""
+        polls = N.CLOSURE_WAIT_DEFAULT if polls is None else int(polls)
+        N.check(N.lib().lbman_closure_set_wait_limit(self._h, polls))
+
     def step(self, coarse, n: int = 1):
         N.check(N.lib().lbman_closure_step(self._h, coarse.handle, int(n)))

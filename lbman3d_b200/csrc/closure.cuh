@@ -17,6 +17,13 @@
 //
 // Tap index: tap = (dz+1)*9 + (dy+1)*3 + (dx+1); output cell c reads input
 // cell c + (dx, dy, dz) with periodic wrap on every axis.
+//
+// Waits: every wait for MMA completion that the pipeline needs to go on
+// polls at most wait_limit times (a kernel argument; tc::kWaitLimit unless
+// the caller lowered it).  A wait that gives up sets *err, the whole CTA
+// leaves its tile loop together (__syncthreads_or), and the drain waits --
+// always with the full tc::kWaitLimit, because the tensor core must finish
+// every MMA it was given before the CTA frees its TMEM -- end the kernel.
 #pragma once
 
 #include <cuda_bf16.h>
@@ -82,7 +89,8 @@ __global__ void __launch_bounds__(kThreads) conv_kernel(Grid3 g, const __nv_bflo
                                                         const __nv_bfloat16* __restrict__ pre_below,
                                                         __nv_bfloat16* __restrict__ out_pre,
                                                         __nv_bfloat16* __restrict__ out_bf, float* __restrict__ out_f,
-                                                        int halo, int* __restrict__ err) {
+                                                        int halo, int* __restrict__ err,
+        uint32_t wait_limit) {
     constexpr int KS = CIN / 16;                 // k-steps per tap
     constexpr int BBYTES = bimg_bytes(CIN, COUT);
     constexpr int ABYTES = KS * 4096;            // one A stage
@@ -140,7 +148,7 @@ __global__ void __launch_bounds__(kThreads) conv_kernel(Grid3 g, const __nv_bflo
         for (int tap = 0; tap < 27; ++tap, ++kt) {
             const int s = kt % kStages;
             // stage s is free once the MMAs that read it last have completed
-            bool lost = uses[s] > 0 && !tc::mbar_wait(&bar[s], (uses[s] - 1) & 1, err);
+            bool lost = uses[s] > 0 && !tc::mbar_wait(&bar[s], (uses[s] - 1) & 1, err, wait_limit);
             if (__syncthreads_or(lost)) {
                 ok = false;
                 break;
@@ -179,7 +187,7 @@ __global__ void __launch_bounds__(kThreads) conv_kernel(Grid3 g, const __nv_bflo
         }
         if (!ok) break;
         // the tile's last commit covers every MMA issued before it
-        const bool lost = !tc::mbar_wait(&bar[last_s], (uses[last_s] - 1) & 1, err);
+        const bool lost = !tc::mbar_wait(&bar[last_s], (uses[last_s] - 1) & 1, err, wait_limit);
         if (__syncthreads_or(lost)) {
             ok = false;
             break;
@@ -315,7 +323,8 @@ __global__ void __launch_bounds__(kThreads) conv_dhalo_kernel(Grid3 g, const __n
                                                               const __nv_bfloat16* __restrict__ pre_below,
                                                               __nv_bfloat16* __restrict__ out_pre,
                                                               __nv_bfloat16* __restrict__ out_bf,
-                                                              float* __restrict__ out_f, int* __restrict__ err) {
+                                                              float* __restrict__ out_f, int* __restrict__ err,
+        uint32_t wait_limit) {
     constexpr int KS = CIN / 16;
     constexpr int BBYTES = bimg_bytes(CIN, COUT);
     constexpr int HB = dhalo_bytes(CIN);
@@ -379,7 +388,7 @@ __global__ void __launch_bounds__(kThreads) conv_dhalo_kernel(Grid3 g, const __n
         // stage the next tile's halo in the other buffer once the MMAs that
         // read it (tile n-1) are done -- that wait also covers the pending epilogue
         const int64_t next = tile + gridDim.x;
-        bool lost = uses[b ^ 1] > 0 && !tc::mbar_wait(&bar[b ^ 1], (uses[b ^ 1] - 1) & 1, err);
+        bool lost = uses[b ^ 1] > 0 && !tc::mbar_wait(&bar[b ^ 1], (uses[b ^ 1] - 1) & 1, err, wait_limit);
         if (__syncthreads_or(lost)) {
             ok = false;
             break;
@@ -405,7 +414,7 @@ __global__ void __launch_bounds__(kThreads) conv_dhalo_kernel(Grid3 g, const __n
     }
     if (ok && prev >= 0) {
         const int b = (n - 1) & 1;
-        const bool lost = !tc::mbar_wait(&bar[b], (uses[b] - 1) & 1, err);
+        const bool lost = !tc::mbar_wait(&bar[b], (uses[b] - 1) & 1, err, wait_limit);
         if (!__syncthreads_or(lost)) {
             tc::fence_after_sync();
             int px, py, pz;
@@ -443,7 +452,8 @@ struct WGradShape {
 template <int CIN, int COUT>
 __global__ void __launch_bounds__(kThreads) wgrad_kernel(Grid3 g, const __nv_bfloat16* __restrict__ act,
                                                          const __nv_bfloat16* __restrict__ grad,
-                                                         float* __restrict__ partials, int* __restrict__ err) {
+                                                         float* __restrict__ partials, int* __restrict__ err,
+        uint32_t wait_limit) {
     using WS = WGradShape<CIN, COUT>;
     constexpr int TPG = WS::TPG, G = WS::G, KC = WS::KC;
     extern __shared__ __align__(1024) unsigned char sm[];
@@ -470,7 +480,7 @@ __global__ void __launch_bounds__(kThreads) wgrad_kernel(Grid3 g, const __nv_bfl
     bool first = true;
     for (int64_t ch = ch0; ch < ch1; ++ch) {
         const int s = (int)((ch - ch0) & 1);
-        bool lost = uses[s] > 0 && !tc::mbar_wait(&bar[s], (uses[s] - 1) & 1, err);
+        bool lost = uses[s] > 0 && !tc::mbar_wait(&bar[s], (uses[s] - 1) & 1, err, wait_limit);
         if (__syncthreads_or(lost)) {
             ok = false;
             break;
@@ -527,7 +537,7 @@ __global__ void __launch_bounds__(kThreads) wgrad_kernel(Grid3 g, const __nv_bfl
     }
     if (ok && uses[0] + uses[1] > 0) {
         const int last = (int)(((ch1 - ch0) - 1) & 1);
-        const bool lost = !tc::mbar_wait(&bar[last], (uses[last] - 1) & 1, err);
+        const bool lost = !tc::mbar_wait(&bar[last], (uses[last] - 1) & 1, err, wait_limit);
         ok = !__syncthreads_or(lost);
     }
     tc::fence_after_sync();
@@ -583,7 +593,8 @@ struct WGradHalo {
 template <int CIN, int COUT>
 __global__ void __launch_bounds__(kThreads) wgrad_dhalo_kernel(Grid3 g, const __nv_bfloat16* __restrict__ act,
                                                                const __nv_bfloat16* __restrict__ grad,
-                                                               float* __restrict__ partials, int* __restrict__ err) {
+                                                               float* __restrict__ partials, int* __restrict__ err,
+        uint32_t wait_limit) {
     using WH = WGradHalo<CIN, COUT>;
     constexpr int TPG = WH::TPG, G = WH::G, QU = CIN / 8;
     extern __shared__ __align__(1024) unsigned char sm[];
@@ -615,7 +626,7 @@ __global__ void __launch_bounds__(kThreads) wgrad_dhalo_kernel(Grid3 g, const __
         const int x0 = (int)(tile % bx) * 8, y0 = (int)((tile / bx) % by) * 16;
         const int z0 = (int)(tile / ((int64_t)bx * by));
         // the previous tile's MMAs read the gradient tile: let them finish
-        bool lost = last_b >= 0 && !tc::mbar_wait(&bar[last_b], (uses[last_b] - 1) & 1, err);
+        bool lost = last_b >= 0 && !tc::mbar_wait(&bar[last_b], (uses[last_b] - 1) & 1, err, wait_limit);
         if (__syncthreads_or(lost)) {
             ok = false;
             break;
@@ -632,7 +643,7 @@ __global__ void __launch_bounds__(kThreads) wgrad_dhalo_kernel(Grid3 g, const __
         __syncthreads();
         for (int gi = 0; gi < G; ++gi, ++kg_run) {
             const int b = kg_run & 1;
-            lost = uses[b] > 0 && !tc::mbar_wait(&bar[b], (uses[b] - 1) & 1, err);
+            lost = uses[b] > 0 && !tc::mbar_wait(&bar[b], (uses[b] - 1) & 1, err, wait_limit);
             if (__syncthreads_or(lost)) {
                 ok = false;
                 break;
@@ -668,7 +679,7 @@ __global__ void __launch_bounds__(kThreads) wgrad_dhalo_kernel(Grid3 g, const __
         any = true;
     }
     if (ok && last_b >= 0) {
-        const bool lost = !tc::mbar_wait(&bar[last_b], (uses[last_b] - 1) & 1, err);
+        const bool lost = !tc::mbar_wait(&bar[last_b], (uses[last_b] - 1) & 1, err, wait_limit);
         ok = !__syncthreads_or(lost);
     }
     tc::fence_after_sync();

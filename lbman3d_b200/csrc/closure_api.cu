@@ -102,6 +102,7 @@ struct lbman_closure {
     float* scales = nullptr;  // shift[9] inv_scale[9] out_scale[8] inv_out_scale[8]
     float h_shift[9], h_scale[9], h_out[8];
     int* err = nullptr;
+    uint32_t wait_limit = lbman::tc::kWaitLimit;  // polls of a pipeline wait before it gives up
     int Gw = 148, Gb = 296;
     std::vector<float*> snaps;
     std::vector<int> traj;
@@ -126,7 +127,7 @@ int run_conv(lbman_closure* c, cudaStream_t st, const __nv_bfloat16* in, const _
         const int grid = (int)std::min<int64_t>(tiles, (int64_t)resident<K>(cl::kThreads, smem) * c->num_sms);
         const cl::Grid3 gr{c->nx, c->ny, c->nz, c->V};
         K<<<grid, cl::kThreads, smem, st>>>(gr, in, reinterpret_cast<const uint4*>(img), bias, pre_below, out_pre,
-                                            out_bf, out_f, c->err);
+                                            out_bf, out_f, c->err, c->wait_limit);
         CL_CUDA(cudaGetLastError());
         return LBMAN_OK;
     }
@@ -139,7 +140,7 @@ int run_conv(lbman_closure* c, cudaStream_t st, const __nv_bfloat16* in, const _
     const int grid = (int)std::min<int64_t>(tiles, (int64_t)resident<K>(cl::kThreads, smem) * c->num_sms);
     const cl::Grid3 gr{c->nx, c->ny, c->nz, c->V};
     K<<<grid, cl::kThreads, smem, st>>>(gr, in, reinterpret_cast<const uint4*>(img), bias, pre_below, out_pre, out_bf,
-                                        out_f, halo, c->err);
+                                        out_f, halo, c->err, c->wait_limit);
     CL_CUDA(cudaGetLastError());
     return LBMAN_OK;
 }
@@ -151,12 +152,12 @@ int run_wgrad(lbman_closure* c, cudaStream_t st, const __nv_bfloat16* a, const _
         using WH = cl::WGradHalo<CIN, COUT>;
         constexpr auto K = cl::wgrad_dhalo_kernel<CIN, COUT>;
         CL_CUDA(cudaFuncSetAttribute(K, cudaFuncAttributeMaxDynamicSharedMemorySize, WH::SMEM));
-        K<<<c->Gw, cl::kThreads, WH::SMEM, st>>>(g3, a, gr, c->wpart, c->err);
+        K<<<c->Gw, cl::kThreads, WH::SMEM, st>>>(g3, a, gr, c->wpart, c->err, c->wait_limit);
     } else {
         using WS = cl::WGradShape<CIN, COUT>;
         constexpr auto K = cl::wgrad_kernel<CIN, COUT>;
         CL_CUDA(cudaFuncSetAttribute(K, cudaFuncAttributeMaxDynamicSharedMemorySize, WS::SMEM));
-        K<<<c->Gw, cl::kThreads, WS::SMEM, st>>>(g3, a, gr, c->wpart, c->err);
+        K<<<c->Gw, cl::kThreads, WS::SMEM, st>>>(g3, a, gr, c->wpart, c->err, c->wait_limit);
     }
     CL_CUDA(cudaGetLastError());
     const int n = 27 * CIN * COUT;
@@ -644,6 +645,14 @@ int lbman_closure_train(lbman_closure* c, int iters, float lr, uint64_t seed, do
     }
     if (loss_first) *loss_first = a / w;
     if (loss_last) *loss_last = b / w;
+    return LBMAN_OK;
+}
+
+static_assert(LBMAN_CLOSURE_WAIT_DEFAULT == lbman::tc::kWaitLimit, "the header's default is the kernels' limit");
+
+int lbman_closure_set_wait_limit(lbman_closure* c, uint32_t polls) {
+    if (!c) return failc(LBMAN_ERR_ARG, "closure: null handle");
+    c->wait_limit = polls;
     return LBMAN_OK;
 }
 

@@ -1,5 +1,6 @@
 """Build recipe for oracle/_ref: the reference's own CPU solver, compiled from
-its sources where they lie under /root/reference (never copied), with a
+its sources where they lie (never copied; the reference's src/ directory is
+taken from $LBMAN_REFERENCE_SRC, by default /root/reference/src), with a
 generated params.h/sim_config.h first on the include path -- the shadowing
 the reference's own tests use (tests/CMakeLists.txt:3-8).
 
@@ -25,7 +26,7 @@ import subprocess
 import sys
 
 HERE = os.path.dirname(os.path.abspath(__file__))
-REF_SRC = "/root/reference/src"
+REF_SRC = os.environ.get("LBMAN_REFERENCE_SRC", "/root/reference/src")
 OUT = os.path.join(HERE, "_ref")
 
 # Physics defaults of src/params.h:36-112.
@@ -46,6 +47,7 @@ REF_BUILDS = {
     "b_slit": dict(nx=64, ny=256, nz=256, ALPHA=0.01),
     "b_channel": dict(nx=20, ny=100, nz=100, ALPHA=0.01),
     "b_p32": dict(nx=32, ny=32, nz=32),
+    "b_p512": dict(nx=512, ny=512, nz=512, ALPHA=0.01),
 }
 
 # Parameter sets of the C++ drop-in check (dropin_check.cc, linked against
@@ -132,12 +134,16 @@ def build(tag: str, cfg: dict, verbose: bool = False) -> str:
     with open(os.path.join(d, "config.json"), "w") as fh:
         json.dump(dict(DEFAULTS, **cfg), fh, indent=1, sort_keys=True)
     exe = os.path.join(d, "ref_driver")
+    # The project's seeded initial condition (orc_seeded_q), for the bench mode.
+    gen = os.path.join(d, "lbman_oracle.o")
+    subprocess.run(["gcc", "-std=c11", "-O2", "-ffp-contract=off", "-fopenmp", "-c", os.path.join(HERE, "lbman_oracle.c"),
+                    "-o", gen], check=True)
     srcs = [os.path.join(HERE, "ref_driver.cc")] + [
         os.path.join(REF_SRC, s) for s in
         ("fluid_fields.cc", "qtensor_fields.cc", "analysis_fields.cc", "analysis/defect_fields.cc")]
     # The reference's release flags (CMakeLists.txt:59-60).
     cmd = ["g++", "-std=c++23", "-O3", "-DNDEBUG", "-fopenmp", "-w",
-           "-I", d, "-I", REF_SRC, "-o", exe] + srcs
+           "-I", d, "-I", REF_SRC, "-I", HERE, "-o", exe] + srcs + [gen, "-lm"]
     if verbose:
         print(" ".join(cmd))
     subprocess.run(cmd, check=True)

@@ -718,6 +718,8 @@ void orc_seeded_q(const orc_params* p, uint64_t seed, double S0, double sigma, d
     const int64_t V = (int64_t)p->nx * p->ny * p->nz;
     const uint64_t key = splitmix64(seed ^ 0x5851f42d4c957f2dULL);
     const double two_pi = 6.283185307179586476925286766559;
+    /* Each cell depends on (seed, cell) only: any thread split gives the same field. */
+#pragma omp parallel for schedule(static)
     for (int64_t c = 0; c < V; ++c) {
         const double ct = 2.0 * uni(key, (uint64_t)c, 0) - 1.0;
         const double ph = two_pi * uni(key, (uint64_t)c, 1);

@@ -18,7 +18,7 @@
 //
 // Usage:
 //   ref_driver <bc> <mode> <in.bin> <out.bin> <snap1> [snap2 ...]
-//   ref_driver --bench <bc> <warmup> <steps>
+//   ref_driver --bench <bc> <seed> <S0> <sigma> <warmup> <steps>
 // mode: full | q | q_active | lbm
 // in.bin : int64 V, int32 has_f, int32 has_force, rho[V] u[3V] q[5V]
 //          [f[15V] direction-major] [force[3V]]   (float64, little endian)
@@ -40,6 +40,7 @@
 #include <vector>
 
 #include "analysis/defect_finder.h"
+#include "lbman_oracle.h"
 #include "analysis_fields.h"
 #include "fluid_fields.h"
 #include "lbm_solver.h"
@@ -270,32 +271,31 @@ int run(const std::string& mode, const char* in_path, const char* out_path,
 }
 
 // Timing loop of src/benchmark.cc:21-50 (std::chrono around each full step),
-// on the project's seeded initial condition supplied in in.bin.
+// on the project's seeded initial condition (rho = 1, u = 0, Q from
+// orc_seeded_q of oracle/lbman_oracle.c, the generator every workload of this
+// project uses), generated in-process so large boxes need no input file.
 template <typename BC>
-int bench(const char* in_path, int warmup, int steps) {
-    FILE* fin = std::fopen(in_path, "rb");
-    if (!fin) throw std::runtime_error("cannot open input");
-    int64_t V = 0; int32_t hf = 0, hF = 0;
-    if (std::fread(&V, 8, 1, fin) != 1 || std::fread(&hf, 4, 1, fin) != 1 || std::fread(&hF, 4, 1, fin) != 1)
-        throw std::runtime_error("bad header");
-    if (V != static_cast<int64_t>(nx) * ny * nz) throw std::runtime_error("grid size mismatch with params.h");
+int bench(uint64_t seed, double S0, double sigma, int warmup, int steps) {
+    const int64_t V = static_cast<int64_t>(nx) * ny * nz;
     g_V = V;
-    g_rho.resize(V); g_u.resize(3 * V); g_q.resize(5 * V);
-    if (std::fread(g_rho.data(), 8, V, fin) != static_cast<size_t>(V) ||
-        std::fread(g_u.data(), 8, 3 * V, fin) != static_cast<size_t>(3 * V) ||
-        std::fread(g_q.data(), 8, 5 * V, fin) != static_cast<size_t>(5 * V))
-        throw std::runtime_error("short input");
-    std::fclose(fin);
+    {
+        orc_params op;
+        std::memset(&op, 0, sizeof(op));
+        op.nx = nx; op.ny = ny; op.nz = nz;
+        g_q.resize(5 * V);
+        orc_seeded_q(&op, seed, S0, sigma, g_q.data());
+    }
     LocalGrid grid = LocalGrid::SingleRank();
     FluidFields ff(grid);
     QTensorFields qf(grid);
     LbmSolver<BC> lbm;
     InjectedSolver<BC, true> qs;
     for (int64_t c = 0; c < V; ++c) {
-        ff.rho[c] = g_rho[c]; ff.ux[c] = g_u[c]; ff.uy[c] = g_u[V + c]; ff.uz[c] = g_u[2 * V + c];
+        ff.rho[c] = 1.0; ff.ux[c] = 0.0; ff.uy[c] = 0.0; ff.uz[c] = 0.0;
     }
     lbm.Initialize(ff);
     qs.Initialize(qf);
+    std::vector<double>().swap(g_q);  // the solver holds its own copy now
     using clock = std::chrono::high_resolution_clock;
     for (int t = 0; t < warmup; ++t) { qs.Step(qf, ff); lbm.LatticeBoltzmannStep(ff); }
     double ms_q = 0, ms_l = 0;
@@ -336,10 +336,11 @@ int dispatch(const std::string& bc, F&& f) {
 int main(int argc, char** argv) {
     try {
         if (argc >= 2 && std::string(argv[1]) == "--bench") {
-            if (argc != 6) throw std::runtime_error("usage: --bench <bc> <in.bin> <warmup> <steps>");
-            const char* in = argv[3];
-            const int w = std::atoi(argv[4]), s = std::atoi(argv[5]);
-            return dispatch(argv[2], [&]<typename BC>() { return bench<BC>(in, w, s); });
+            if (argc != 8) throw std::runtime_error("usage: --bench <bc> <seed> <S0> <sigma> <warmup> <steps>");
+            const uint64_t seed = std::strtoull(argv[3], nullptr, 10);
+            const double S0 = std::atof(argv[4]), sigma = std::atof(argv[5]);
+            const int w = std::atoi(argv[6]), s = std::atoi(argv[7]);
+            return dispatch(argv[2], [&]<typename BC>() { return bench<BC>(seed, S0, sigma, w, s); });
         }
         if (argc < 6) throw std::runtime_error("usage: ref_driver <bc> <mode> <in.bin> <out.bin> <snap>...");
         std::vector<int64_t> snaps;

@@ -43,6 +43,30 @@ def test_forward_matches_oracle(grid):
     assert np.max(np.abs(got - ref)) <= 2e-2 * np.max(np.abs(ref))
 
 
+# (8, 8, 8): the gather convolution and weight-gradient kernels; (16, 16, 8):
+# the descriptor-halo forms.  A limit of 0 polls makes the first completion
+# wait of every CTA give up while its MMAs still run to completion, so the
+# timeout path is exercised without a fault: the call must report
+# LBMAN_ERR_TIMEOUT, and the next call at the default limit must give the
+# same outputs and gradients as before.
+@pytest.mark.parametrize("grid", [(8, 8, 8), (16, 16, 8)])
+def test_wait_that_gives_up_reports_timeout_and_next_call_recovers(grid):
+    feat, tgt = _case(grid, 3)
+    with CL.Closure(*grid, seed=7) as cl:
+        out0 = cl.forward(feat)
+        loss0, g0 = cl.gradient(feat, tgt)
+        cl.set_wait_limit(0)
+        for call in (lambda: cl.forward(feat), lambda: cl.gradient(feat, tgt)):
+            with pytest.raises(L._native.LbmanError) as e:
+                call()
+            assert e.value.status == L._native.ERR_TIMEOUT
+        cl.set_wait_limit()
+        np.testing.assert_array_equal(cl.forward(feat), out0)
+        loss1, g1 = cl.gradient(feat, tgt)
+        assert loss1 == loss0
+        np.testing.assert_array_equal(g1, g0)
+
+
 @pytest.mark.parametrize("grid", [(8, 8, 8), (5, 6, 7), (16, 16, 8)])
 def test_gradient_matches_oracle(grid):
     feat, tgt = _case(grid, 2)
