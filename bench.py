@@ -48,6 +48,9 @@ WORKLOADS = {
     "slit64": (64, 256, 256, "slit", 0.01, "b_slit"),
     "channel20": (20, 100, 100, "channel", 0.01, "b_channel"),
     "periodic32": (32, 32, 32, "periodic", 0.023, "b_p32"),
+    # a 512^2 x 64 slab of the precision configuration: profiler captures
+    # (a few GB on the device), scaled per cell to the full box
+    "periodic512x64": (512, 512, 64, "periodic", 0.01, None),
 }
 SEED, S0, SIGMA = 1234, 0.5, 1e-3
 # Host bytes per cell of the reference's CPU solver: FluidFields (f, f_new,

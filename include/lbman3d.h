@@ -149,6 +149,25 @@ int lbman_qtensor_step(lbman_solver* s);
  * force (src/cuda/device_solver.cu:101-121).                                 */
 int lbman_lbm_step(lbman_solver* s);
 
+/* The Q stage as the reference's two phases, for callers that replace the
+ * activity model between them (a subclass overriding the virtual
+ * QTensorSolver::SetActiveStressAndComputeBodyForce, src/qtensor_solver.h:
+ * 11-21, 48).  lbman_qtensor_step does both in one pass.
+ *   lbman_qtensor_setup  <- QTensorSolver::StepAndSetupBodyForce
+ *                           (src/qtensor_solver.tpp:51-147): Q := Q_new, the
+ *                           stresses Sigma (5) and tau (3) kept on the device,
+ *                           body force := the Ericksen seed.
+ *   lbman_active_force   <- the base SetActiveStressAndComputeBodyForce
+ *                           (src/qtensor_solver.tpp:155-217): body force +=
+ *                           -ALPHA div Q + div(Sigma + tau) - MU u.
+ *   lbman_download_stress / lbman_upload_stress: Sigma [5V] (xx xy xz yy yz)
+ *                           and tau [3V] (xy xz yz), FP64 host arrays
+ *                           (QTensorFields::Sigma_* / Tau_*).               */
+int lbman_qtensor_setup(lbman_solver* s);
+int lbman_active_force(lbman_solver* s);
+int lbman_download_stress(lbman_solver* s, double* sigma5, double* tau3);
+int lbman_upload_stress(lbman_solver* s, const double* sigma5, const double* tau3);
+
 /* SimIO::Log reductions + TotalNematicFreeEnergy + defect plaquettes, FP64
  * accumulation on the device.  Returns LBMAN_ERR_DIVERGED (after filling out)
  * when the mass or momentum is NaN, as SimIO::Log returns false.            */

@@ -34,6 +34,7 @@
 #include <stdexcept>
 #include <string>
 #include <type_traits>
+#include <typeinfo>
 #include <vector>
 
 #include "boundary.h"
@@ -265,16 +266,45 @@ public:
     }
 };
 
-// GPU-backed QTensorSolver<BC> (src/qtensor_solver.h:23-52).  One GPU pass
-// computes what the reference's StepAndSetupBodyForce followed by the base
-// SetActiveStressAndComputeBodyForce computes, and writes the new Q and the
-// full body force back to the host fields.  As in the reference's own GPU
-// path (src/active_nematic.h:85-86), an override of
-// SetActiveStressAndComputeBodyForce does not replace the built-in activity
-// model: it runs after the pass, on the full force.
+// GPU-backed QTensorSolver<BC> (src/qtensor_solver.h:23-52) with the
+// reference's two-phase contract: StepAndSetupBodyForce writes Q_new (after
+// the swap of src/qtensor_solver.tpp:150-152), Sigma, tau and the Ericksen
+// seed of the body force to the host fields; the virtual
+// SetActiveStressAndComputeBodyForce then adds the active, passive and
+// friction terms, and a subclass override replaces it as in the reference
+// (src/qtensor_solver.h:11-21).  Step runs the two phases, except for an
+// object of exactly this class (no subclass, so no override), where one GPU
+// pass computes the same Q and force; that pass does not refresh
+// qf.Sigma_* / qf.Tau_*, which nothing but the second phase reads.
 template <typename BC>
 class QTensorSolver {
     mutable lbman_solver* s_ = nullptr;
+
+    lbman_solver* get(const LocalGrid& g) const {
+        if (!s_) {
+            lbman_config cfg = lbman_dropin::make_config<BC>(g);
+            cfg.kernels = LBMAN_KERNELS_SPLIT;
+            lbman_dropin::check(lbman_create(&cfg, &s_));
+        }
+        return s_;
+    }
+    static int64_t volume(const LocalGrid& g) { return (int64_t)g.local_nx * g.local_ny * g.local_nz; }
+
+    // new Q (q5) into qf, the previous Q into qf.*_new, as SwapWithNew leaves them
+    static void store_q(QTensorFields& qf, const std::vector<double>& q5, int64_t V) {
+        std::vector<double>* cur[5] = {&qf.qxx, &qf.qxy, &qf.qxz, &qf.qyy, &qf.qyz};
+        std::vector<double>* old[5] = {&qf.qxx_new, &qf.qxy_new, &qf.qxz_new, &qf.qyy_new, &qf.qyz_new};
+        for (int k = 0; k < 5; ++k)
+            for (int64_t c = 0; c < V; ++c) {
+                (*old[k])[c] = (*cur[k])[c];
+                (*cur[k])[c] = q5[k * V + c];
+            }
+    }
+    static void store_force(FluidFields& ff, const std::vector<double>& F3, int64_t V) {
+        for (int64_t c = 0; c < V; ++c) {
+            ff.fx[c] = F3[c]; ff.fy[c] = F3[V + c]; ff.fz[c] = F3[2 * V + c];
+        }
+    }
 
 public:
     QTensorSolver() = default;
@@ -292,8 +322,7 @@ public:
         std::random_device rd;
         std::mt19937 gen(rd());
         std::uniform_real_distribution<double> noise(-Params::NOISE, Params::NOISE);
-        const LocalGrid& g = qf.grid;
-        const int64_t V = (int64_t)g.local_nx * g.local_ny * g.local_nz;
+        const int64_t V = volume(qf.grid);
         for (int64_t c = 0; c < V; ++c) {
             qf.qxx[c] = -s_eq / 3.0 + noise(gen);
             qf.qxy[c] = noise(gen);
@@ -303,33 +332,69 @@ public:
         }
     }
 
-    void StepAndSetupBodyForce(QTensorFields& qf, FluidFields& ff) const { StepFused(qf, ff); }
-    virtual void SetActiveStressAndComputeBodyForce(FluidFields&, const QTensorFields&) const {}
+    // Phase 1 (src/qtensor_solver.tpp:51-147) on the GPU.
+    void StepAndSetupBodyForce(QTensorFields& qf, FluidFields& ff) const {
+        const int64_t V = volume(qf.grid);
+        lbman_solver* s = get(qf.grid);
+        lbman_dropin::Staging st;
+        st.from_fields(ff, qf, V);
+        lbman_dropin::check(lbman_upload(s, ff.rho.data(), st.u3.data(), st.q5.data(), nullptr, nullptr));
+        lbman_dropin::check(lbman_qtensor_setup(s));
+        std::vector<double> sig(5 * V), tau(3 * V);
+        lbman_dropin::check(lbman_download(s, nullptr, nullptr, st.q5.data(), nullptr, st.F3.data()));
+        lbman_dropin::check(lbman_download_stress(s, sig.data(), tau.data()));
+        store_q(qf, st.q5, V);
+        store_force(ff, st.F3, V);
+        std::vector<double>* S[5] = {&qf.Sigma_xx, &qf.Sigma_xy, &qf.Sigma_xz, &qf.Sigma_yy, &qf.Sigma_yz};
+        std::vector<double>* T[3] = {&qf.Tau_xy, &qf.Tau_xz, &qf.Tau_yz};
+        for (int64_t c = 0; c < V; ++c) {
+            for (int k = 0; k < 5; ++k) (*S[k])[c] = sig[k * V + c];
+            for (int k = 0; k < 3; ++k) (*T[k])[c] = tau[k * V + c];
+        }
+    }
+
+    // Phase 2, the base activity model (src/qtensor_solver.tpp:155-217), on
+    // the GPU: ff.f* += -ALPHA div Q + div(Sigma + tau) - MU u.
+    virtual void SetActiveStressAndComputeBodyForce(FluidFields& ff, const QTensorFields& qf) const {
+        const int64_t V = volume(qf.grid);
+        lbman_solver* s = get(qf.grid);
+        lbman_dropin::Staging st;
+        st.from_fields(ff, qf, V);
+        std::vector<double> sig(5 * V), tau(3 * V);
+        const std::vector<double>* S[5] = {&qf.Sigma_xx, &qf.Sigma_xy, &qf.Sigma_xz, &qf.Sigma_yy, &qf.Sigma_yz};
+        const std::vector<double>* T[3] = {&qf.Tau_xy, &qf.Tau_xz, &qf.Tau_yz};
+        for (int64_t c = 0; c < V; ++c) {
+            for (int k = 0; k < 5; ++k) sig[k * V + c] = (*S[k])[c];
+            for (int k = 0; k < 3; ++k) tau[k * V + c] = (*T[k])[c];
+        }
+        lbman_dropin::check(lbman_upload(s, ff.rho.data(), st.u3.data(), st.q5.data(), nullptr, st.F3.data()));
+        lbman_dropin::check(lbman_upload_stress(s, sig.data(), tau.data()));
+        lbman_dropin::check(lbman_active_force(s));
+        lbman_dropin::check(lbman_download(s, nullptr, nullptr, nullptr, nullptr, st.F3.data()));
+        store_force(ff, st.F3, V);
+    }
 
     void Step(QTensorFields& qf, FluidFields& ff) const {
-        StepFused(qf, ff);
+        if (typeid(*this) == typeid(QTensorSolver)) {
+            StepFused(qf, ff);
+            return;
+        }
+        StepAndSetupBodyForce(qf, ff);
         SetActiveStressAndComputeBodyForce(ff, qf);
     }
 
 private:
+    // Both phases of the base class in one GPU pass (lbman_qtensor_step).
     void StepFused(QTensorFields& qf, FluidFields& ff) const {
-        const LocalGrid& g = qf.grid;
-        const int64_t V = (int64_t)g.local_nx * g.local_ny * g.local_nz;
-        if (!s_) {
-            lbman_config cfg = lbman_dropin::make_config<BC>(g);
-            cfg.kernels = LBMAN_KERNELS_SPLIT;
-            lbman_dropin::check(lbman_create(&cfg, &s_));
-        }
+        const int64_t V = volume(qf.grid);
+        lbman_solver* s = get(qf.grid);
         lbman_dropin::Staging st;
         st.from_fields(ff, qf, V);
-        lbman_dropin::check(lbman_upload(s_, ff.rho.data(), st.u3.data(), st.q5.data(), nullptr, nullptr));
-        lbman_dropin::check(lbman_qtensor_step(s_));
-        lbman_dropin::check(lbman_download(s_, nullptr, nullptr, st.q5.data(), nullptr, st.F3.data()));
-        for (int64_t c = 0; c < V; ++c) {
-            qf.qxx[c] = st.q5[c]; qf.qxy[c] = st.q5[V + c]; qf.qxz[c] = st.q5[2 * V + c];
-            qf.qyy[c] = st.q5[3 * V + c]; qf.qyz[c] = st.q5[4 * V + c];
-            ff.fx[c] = st.F3[c]; ff.fy[c] = st.F3[V + c]; ff.fz[c] = st.F3[2 * V + c];
-        }
+        lbman_dropin::check(lbman_upload(s, ff.rho.data(), st.u3.data(), st.q5.data(), nullptr, nullptr));
+        lbman_dropin::check(lbman_qtensor_step(s));
+        lbman_dropin::check(lbman_download(s, nullptr, nullptr, st.q5.data(), nullptr, st.F3.data()));
+        store_q(qf, st.q5, V);
+        store_force(ff, st.F3, V);
     }
 };
 

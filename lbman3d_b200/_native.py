@@ -93,6 +93,10 @@ PROTOTYPES = [
     ("lbman_step", C.c_int, [C.c_void_p, C.c_int]),
     ("lbman_qtensor_step", C.c_int, [C.c_void_p]),
     ("lbman_lbm_step", C.c_int, [C.c_void_p]),
+    ("lbman_qtensor_setup", C.c_int, [C.c_void_p]),
+    ("lbman_active_force", C.c_int, [C.c_void_p]),
+    ("lbman_download_stress", C.c_int, [C.c_void_p, _DP, _DP]),
+    ("lbman_upload_stress", C.c_int, [C.c_void_p, _DP, _DP]),
     ("lbman_reduce", C.c_int, [C.c_void_p, C.c_int, C.POINTER(lbman_diag)]),
     ("lbman_steps_done", C.c_int, [C.c_void_p, C.POINTER(C.c_int64)]),
     ("lbman_launch_count", C.c_int, [C.c_void_p, C.POINTER(C.c_int64)]),

@@ -62,6 +62,8 @@ struct Ops {
     decltype(&launch_defect_count_f64) defect_count;
     decltype(&launch_defect_flags_f64) defect_flags;
     decltype(&launch_seeded_init_f64) seeded_init;
+    decltype(&launch_qsetup_f64) qsetup;
+    decltype(&launch_active_force_f64) active_force;
     decltype(&qforce_smem_f64) qforce_smem;
     decltype(&qforce_threads_f64) qforce_threads;
     decltype(&march_blocks_f64) march_blocks;
@@ -74,7 +76,7 @@ struct Ops {
             launch_feq_init_##SUF, launch_pop_in_##SUF, launch_pop_out_##SUF, launch_real_in_##SUF,    \
             launch_real_out_##SUF, launch_flow_reduce_##SUF, launch_energy_reduce_##SUF,               \
             launch_director_##SUF, launch_defect_count_##SUF, launch_defect_flags_##SUF,              \
-            launch_seeded_init_##SUF,                                                                  \
+            launch_seeded_init_##SUF, launch_qsetup_##SUF, launch_active_force_##SUF,                  \
             qforce_smem_##SUF, qforce_threads_##SUF, march_blocks_##SUF, prepare_##SUF                 \
     }
 
@@ -145,6 +147,7 @@ struct lbman_solver {
     void* u[2] = {nullptr, nullptr};
     void* rho = nullptr;
     void* F = nullptr;
+    void* stress = nullptr;  // Sigma (5) and tau (3) of the two-phase Q stage, allocated on first use
     double* staging = nullptr;
     double* partials = nullptr;
     int red_G = 0;
@@ -402,7 +405,7 @@ int lbman_destroy(lbman_solver* s) {
     if (s->stream) cudaStreamSynchronize(s->stream);
     for (int b = 0; b < 2; ++b) { cudaFree(s->f[b]); cudaFree(s->q[b]); cudaFree(s->u[b]); }
     cudaFree(s->rho); cudaFree(s->F); cudaFree(s->staging); cudaFree(s->partials); cudaFree(s->red_dev);
-    cudaFree(s->upast); cudaFree(s->dirbuf);
+    cudaFree(s->upast); cudaFree(s->dirbuf); cudaFree(s->stress);
     lbman::stats::destroy(s->stats);
     if (s->red_host) cudaFreeHost(s->red_host);
     if (s->own_stream && s->stream) cudaStreamDestroy(s->stream);
@@ -585,6 +588,58 @@ int lbman_qtensor_step(lbman_solver* s) {
     LB_TRY(check_launch(s, s->ops().qforce(s->P, s->shape, s->q[s->qcur], s->u[s->ucur], s->q[1 - s->qcur], s->F, s->stream),
                         "qforce"));
     s->qcur ^= 1;
+    return LBMAN_OK;
+}
+
+static int ensure_stress(lbman_solver* s) {
+    if (!s->stress) LB_CUDA(cudaMalloc(&s->stress, 8 * s->P.V * s->rbytes));
+    return LBMAN_OK;
+}
+
+int lbman_qtensor_setup(lbman_solver* s) {
+    if (!s) return fail(LBMAN_ERR_ARG, "null solver");
+    if (!s->uploaded) return fail(LBMAN_ERR_STATE, "step before upload");
+    LB_TRY(set_device(s));
+    LB_TRY(ensure_stress(s));
+    const int64_t V = s->P.V;
+    LB_TRY(check_launch(s, s->ops().qsetup(s->P, s->q[s->qcur], s->u[s->ucur], s->q[1 - s->qcur], s->stress,
+                                           vptr(s->stress, 5 * V, s->rbytes), s->F, s->stream),
+                        "qsetup"));
+    s->qcur ^= 1;
+    return LBMAN_OK;
+}
+
+int lbman_active_force(lbman_solver* s) {
+    if (!s) return fail(LBMAN_ERR_ARG, "null solver");
+    if (!s->uploaded) return fail(LBMAN_ERR_STATE, "step before upload");
+    if (!s->stress) return fail(LBMAN_ERR_STATE, "no stress: call lbman_qtensor_setup or lbman_upload_stress first");
+    LB_TRY(set_device(s));
+    const int64_t V = s->P.V;
+    LB_TRY(check_launch(s, s->ops().active_force(s->P, s->q[s->qcur], s->stress, vptr(s->stress, 5 * V, s->rbytes),
+                                                 s->u[s->ucur], s->F, s->stream),
+                        "active_force"));
+    return LBMAN_OK;
+}
+
+int lbman_upload_stress(lbman_solver* s, const double* sigma5, const double* tau3) {
+    if (!s || !sigma5 || !tau3) return fail(LBMAN_ERR_ARG, "null argument");
+    LB_TRY(set_device(s));
+    LB_TRY(ensure_stress(s));
+    const int64_t V = s->P.V;
+    for (int k = 0; k < 5; ++k) LB_TRY(stage_in_real(s, sigma5 + k * V, vptr(s->stress, k * V, s->rbytes), V));
+    for (int k = 0; k < 3; ++k) LB_TRY(stage_in_real(s, tau3 + k * V, vptr(s->stress, (5 + k) * V, s->rbytes), V));
+    LB_CUDA(cudaStreamSynchronize(s->stream));
+    return LBMAN_OK;
+}
+
+int lbman_download_stress(lbman_solver* s, double* sigma5, double* tau3) {
+    if (!s) return fail(LBMAN_ERR_ARG, "null solver");
+    if (!s->stress) return fail(LBMAN_ERR_STATE, "no stress: call lbman_qtensor_setup first");
+    LB_TRY(set_device(s));
+    const int64_t V = s->P.V;
+    if (sigma5) for (int k = 0; k < 5; ++k) LB_TRY(stage_out_real(s, vptr(s->stress, k * V, s->rbytes), sigma5 + k * V, V));
+    if (tau3) for (int k = 0; k < 3; ++k) LB_TRY(stage_out_real(s, vptr(s->stress, (5 + k) * V, s->rbytes), tau3 + k * V, V));
+    LB_CUDA(cudaStreamSynchronize(s->stream));
     return LBMAN_OK;
 }
 

@@ -4,6 +4,7 @@
 
 #include "fused.cuh"
 #include "init.cuh"
+#include "qsplit.cuh"
 #include "launch.h"
 #include "reduce.cuh"
 #include "tiles.h"
@@ -268,6 +269,27 @@ cudaError_t seeded_init(const SimParams& P, uint64_t seed, double S0, double sig
     return cudaGetLastError();
 }
 
+template <class R>
+cudaError_t qsetup(const SimParams& P, const void* qin, const void* uin, void* qout, void* sig, void* tau, void* F,
+                   cudaStream_t st) {
+    const unsigned nb = blocks_for(P.V, 128);
+    if (P.upwind)
+        qsetup_kernel<R, true><<<nb, 128, 0, st>>>(P, (const R*)qin, (const R*)uin, (R*)qout, (R*)sig, (R*)tau,
+                                                   (R*)F);
+    else
+        qsetup_kernel<R, false><<<nb, 128, 0, st>>>(P, (const R*)qin, (const R*)uin, (R*)qout, (R*)sig, (R*)tau,
+                                                    (R*)F);
+    return cudaGetLastError();
+}
+
+template <class R>
+cudaError_t active_force(const SimParams& P, const void* q, const void* sig, const void* tau, const void* u, void* F,
+                         cudaStream_t st) {
+    active_force_kernel<R><<<blocks_for(P.V, 128), 128, 0, st>>>(P, (const R*)q, (const R*)sig, (const R*)tau,
+                                                                 (const R*)u, (R*)F);
+    return cudaGetLastError();
+}
+
 template <class R, class S, bool DEV>
 cudaError_t prepare(size_t max_smem) {
     const int b = (int)max_smem;
@@ -355,6 +377,14 @@ cudaError_t prepare(size_t max_smem) {
     cudaError_t launch_seeded_init_##SUF(const SimParams& P, uint64_t seed, double S0, double sigma,    \
                                          void* rho, void* u, void* q, void* F, cudaStream_t st) {      \
         return impl::seeded_init<R>(P, seed, S0, sigma, rho, u, q, F, st);                              \
+    }                                                                                                   \
+    cudaError_t launch_qsetup_##SUF(const SimParams& P, const void* qin, const void* uin, void* qout,   \
+                                    void* sig, void* tau, void* F, cudaStream_t st) {                  \
+        return impl::qsetup<R>(P, qin, uin, qout, sig, tau, F, st);                                     \
+    }                                                                                                   \
+    cudaError_t launch_active_force_##SUF(const SimParams& P, const void* q, const void* sig,           \
+                                          const void* tau, const void* u, void* F, cudaStream_t st) {  \
+        return impl::active_force<R>(P, q, sig, tau, u, F, st);                                         \
     }                                                                                                   \
     size_t qforce_smem_##SUF(const QTile& T) { return impl::qforce_smem<R>(T); }                       \
     int qforce_threads_##SUF(const QTile& T) { return impl::qforce_threads<R>(T); }                    \

@@ -50,6 +50,10 @@ struct LaunchShape {
                                           cudaStream_t st);                                            \
     cudaError_t launch_seeded_init_##SUF(const SimParams& P, uint64_t seed, double S0, double sigma,    \
                                          void* rho, void* u, void* q, void* F, cudaStream_t st);       \
+    cudaError_t launch_qsetup_##SUF(const SimParams& P, const void* qin, const void* uin, void* qout,   \
+                                    void* sig, void* tau, void* F, cudaStream_t st);                   \
+    cudaError_t launch_active_force_##SUF(const SimParams& P, const void* q, const void* sig,           \
+                                          const void* tau, const void* u, void* F, cudaStream_t st);   \
     size_t qforce_smem_##SUF(const QTile& T);                                                          \
     int qforce_threads_##SUF(const QTile& T);                                                          \
     int march_blocks_##SUF(const SimParams& P, const LaunchShape& shape, bool fused_org);              \

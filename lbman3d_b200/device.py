@@ -117,6 +117,29 @@ class Simulation:
     def lbm_step(self):
         N.check(N.lib().lbman_lbm_step(self._h))
 
+    def qtensor_setup(self):
+        """Phase 1 of the Q stage: Q := Q_new, Sigma and tau kept on the
+        device, body force := the Ericksen seed."""
+        N.check(N.lib().lbman_qtensor_setup(self._h))
+
+    def active_force(self):
+        """Phase 2, the base activity model: force += -ALPHA div Q +
+        div(Sigma + tau) - MU u."""
+        N.check(N.lib().lbman_active_force(self._h))
+
+    def download_stress(self):
+        V = self.V
+        sig, tau = np.empty(5 * V), np.empty(3 * V)
+        N.check(N.lib().lbman_download_stress(self._h, N.dptr(sig), N.dptr(tau)))
+        return sig, tau
+
+    def upload_stress(self, sigma5, tau3):
+        sig = np.ascontiguousarray(sigma5, dtype=np.float64)
+        tau = np.ascontiguousarray(tau3, dtype=np.float64)
+        if sig.size != 5 * self.V or tau.size != 3 * self.V:
+            raise ValueError("sigma needs 5V values and tau 3V")
+        N.check(N.lib().lbman_upload_stress(self._h, N.dptr(sig), N.dptr(tau)))
+
     def synchronize(self):
         N.check(N.lib().lbman_synchronize(self._h))
 
@@ -267,10 +290,18 @@ class LbmSolver:
 
 
 class QTensorSolver:
-    """QTensorSolver<BC> on host fields (src/qtensor_solver.h:23-52).  Step =
-    StepAndSetupBodyForce + SetActiveStressAndComputeBodyForce in one GPU pass;
-    like the reference's GPU path, subclass overrides of the activity model
-    are not consulted on the device."""
+    """QTensorSolver<BC> on host fields (src/qtensor_solver.h:23-52), run on
+    the GPU with the reference's two-phase contract:
+    StepAndSetupBodyForce writes Q_new (Q and Q_new exchanged as SwapWithNew
+    leaves them), Sigma, tau and the Ericksen seed of the body force; the
+    overridable SetActiveStressAndComputeBodyForce adds the active, passive
+    and friction terms, and a subclass override replaces it
+    (src/qtensor_solver.h:11-21).  Step runs both phases; an object of
+    exactly this class (nothing overridden) takes one fused GPU pass, which
+    leaves qf.Sigma_* / qf.Tau_* as they were."""
+
+    SIGMA = ("Sigma_xx", "Sigma_xy", "Sigma_xz", "Sigma_yy", "Sigma_yz")
+    TAU = ("Tau_xy", "Tau_xz", "Tau_yz")
 
     def __init__(self, bc: BCConfig, params: Params, precision: int = Precision.FP64, device: int = 0):
         self.bc, self.params = bc, params
@@ -289,11 +320,42 @@ class QTensorSolver:
         qf.qyy[:] = -s_eq / 3.0 + rng.uniform(-nz, nz, V)
         qf.qyz[:] = rng.uniform(-nz, nz, V)
 
-    def Step(self, qf: QTensorFields, ff: FluidFields):
+    def _store(self, qf: QTensorFields, ff: FluidFields, out):
         V = self.params.V
-        self.sim.upload(ff.rho, ff.u3(), qf.q5())
-        self.sim.qtensor_step()
-        out = self.sim.download(force=True)
-        qf.set_q5(out["q"])
+        for k, c in enumerate(qf.COMPS):
+            getattr(qf, c + "_new")[:] = getattr(qf, c)
+            getattr(qf, c)[:] = out["q"][k * V:(k + 1) * V]
         F = out["force"]
         ff.fx[:], ff.fy[:], ff.fz[:] = F[:V], F[V:2 * V], F[2 * V:]
+
+    def StepAndSetupBodyForce(self, qf: QTensorFields, ff: FluidFields):
+        """Phase 1 (src/qtensor_solver.tpp:51-147) on the GPU."""
+        V = self.params.V
+        self.sim.upload(ff.rho, ff.u3(), qf.q5())
+        self.sim.qtensor_setup()
+        self._store(qf, ff, self.sim.download(force=True))
+        sig, tau = self.sim.download_stress()
+        for k, c in enumerate(self.SIGMA):
+            getattr(qf, c)[:] = sig[k * V:(k + 1) * V]
+        for k, c in enumerate(self.TAU):
+            getattr(qf, c)[:] = tau[k * V:(k + 1) * V]
+
+    def SetActiveStressAndComputeBodyForce(self, ff: FluidFields, qf: QTensorFields):
+        """Phase 2, the base activity model (src/qtensor_solver.tpp:155-217),
+        on the GPU; override to change the activity model."""
+        V = self.params.V
+        self.sim.upload(ff.rho, ff.u3(), qf.q5(), force=ff.force3())
+        self.sim.upload_stress(np.concatenate([getattr(qf, c) for c in self.SIGMA]),
+                               np.concatenate([getattr(qf, c) for c in self.TAU]))
+        self.sim.active_force()
+        F = self.sim.download(force=True)["force"]
+        ff.fx[:], ff.fy[:], ff.fz[:] = F[:V], F[V:2 * V], F[2 * V:]
+
+    def Step(self, qf: QTensorFields, ff: FluidFields):
+        if type(self) is QTensorSolver:
+            self.sim.upload(ff.rho, ff.u3(), qf.q5())
+            self.sim.qtensor_step()
+            self._store(qf, ff, self.sim.download(force=True))
+            return
+        self.StepAndSetupBodyForce(qf, ff)
+        self.SetActiveStressAndComputeBodyForce(ff, qf)

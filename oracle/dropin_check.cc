@@ -15,6 +15,14 @@
 //           fields against LbmSolver<BC> (populations compared too).
 //   q     : lbman::QTensorSolver<BC>::Step against QTensorSolver<BC>::Step
 //           (new Q and the full body force compared).
+//   q_setup : StepAndSetupBodyForce alone (new and previous Q, Sigma, tau,
+//           Ericksen seed compared).
+//   q_zero / q_varying / q_init_only : Step of subclasses written once and
+//           derived from either class -- the empty override the reference
+//           documents for pure relaxation (src/qtensor_solver.h:21), an
+//           override that calls the base and adds a space-varying active
+//           term (the VaryingAlpha pattern, src/qtensor_solver.h:11-19), and
+//           a subclass that overrides only Initialize.
 //
 // Usage: dropin_check <steps>      prints one JSON line per check, exit 0
 //                                  iff every field matched bitwise.
@@ -84,6 +92,35 @@ void fill(FluidFields& ff, QTensorFields& qf) {
         qf.qyz[c] = 0.05 * unit(c, 8);
     }
 }
+
+// Subclasses of the reference's QTensorSolver and of the drop-in, from one
+// source: Base is ::QTensorSolver<BC> or lbman::QTensorSolver<BC>.
+template <class Base>
+struct ZeroActivity : Base {
+    void SetActiveStressAndComputeBodyForce(FluidFields&, const QTensorFields&) const override {}
+};
+template <class Base>
+struct VaryingAlpha : Base {
+    void SetActiveStressAndComputeBodyForce(FluidFields& ff, const QTensorFields& qf) const override {
+        Base::SetActiveStressAndComputeBodyForce(ff, qf);
+        const LocalGrid& g = qf.grid;
+        const int nx = g.local_nx, ny = g.local_ny, nz = g.local_nz;
+        for (int z = 0; z < nz; ++z)
+            for (int y = 0; y < ny; ++y)
+                for (int x = 0; x < nx; ++x) {
+                    const int64_t c = ((int64_t)z * ny + y) * nx + x;
+                    const int64_t xm = c - x + (x + nx - 1) % nx, xp = c - x + (x + 1) % nx;
+                    const double a = 0.01 * std::sin(2.0 * std::numbers::pi * x / nx);
+                    ff.fx[c] += -a * 0.5 * (qf.qxx[xp] - qf.qxx[xm]);
+                    ff.fy[c] += -a * 0.5 * (qf.qxy[xp] - qf.qxy[xm]);
+                    ff.fz[c] += -a * 0.5 * (qf.qxz[xp] - qf.qxz[xm]);
+                }
+    }
+};
+template <class Base>
+struct InitOnly : Base {
+    void Initialize(QTensorFields& qf) const override { Base::Initialize(qf); }
+};
 
 struct Cmp {
     int64_t mismatches = 0;
@@ -196,6 +233,46 @@ void check_bc(int steps, bool& ok) {
         c.add(ffr.fz, ffd.fz, V);
         report("q", BC::name, 1, c, ok);
     }
+    // q_setup: phase 1 alone.
+    {
+        FluidFields ffr(g), ffd(g);
+        QTensorFields qfr(g), qfd(g);
+        fill(ffr, qfr);
+        fill(ffd, qfd);
+        QTensorSolver<BC> ref;
+        lbman::QTensorSolver<BC> gpu;
+        ref.StepAndSetupBodyForce(qfr, ffr);
+        gpu.StepAndSetupBodyForce(qfd, ffd);
+        Cmp c;
+        c.add(qfr.qxx, qfd.qxx, V); c.add(qfr.qxy, qfd.qxy, V); c.add(qfr.qxz, qfd.qxz, V);
+        c.add(qfr.qyy, qfd.qyy, V); c.add(qfr.qyz, qfd.qyz, V);
+        c.add(qfr.qxx_new, qfd.qxx_new, V); c.add(qfr.qyz_new, qfd.qyz_new, V);
+        c.add(qfr.Sigma_xx, qfd.Sigma_xx, V); c.add(qfr.Sigma_xy, qfd.Sigma_xy, V);
+        c.add(qfr.Sigma_xz, qfd.Sigma_xz, V); c.add(qfr.Sigma_yy, qfd.Sigma_yy, V);
+        c.add(qfr.Sigma_yz, qfd.Sigma_yz, V);
+        c.add(qfr.Tau_xy, qfd.Tau_xy, V); c.add(qfr.Tau_xz, qfd.Tau_xz, V); c.add(qfr.Tau_yz, qfd.Tau_yz, V);
+        c.add(ffr.fx, ffd.fx, V); c.add(ffr.fy, ffd.fy, V); c.add(ffr.fz, ffd.fz, V);
+        report("q_setup", BC::name, 1, c, ok);
+    }
+    // Subclasses: Step of each, two steps in a row.
+    auto sub = [&](const char* name, const auto& ref, const auto& gpu) {
+        FluidFields ffr(g), ffd(g);
+        QTensorFields qfr(g), qfd(g);
+        fill(ffr, qfr);
+        fill(ffd, qfd);
+        for (int n = 0; n < 2; ++n) {
+            ref.Step(qfr, ffr);
+            gpu.Step(qfd, ffd);
+        }
+        Cmp c;
+        c.add(qfr.qxx, qfd.qxx, V); c.add(qfr.qxy, qfd.qxy, V); c.add(qfr.qxz, qfd.qxz, V);
+        c.add(qfr.qyy, qfd.qyy, V); c.add(qfr.qyz, qfd.qyz, V);
+        c.add(ffr.fx, ffd.fx, V); c.add(ffr.fy, ffd.fy, V); c.add(ffr.fz, ffd.fz, V);
+        report(name, BC::name, 2, c, ok);
+    };
+    sub("q_zero", ZeroActivity<QTensorSolver<BC>>{}, ZeroActivity<lbman::QTensorSolver<BC>>{});
+    sub("q_varying", VaryingAlpha<QTensorSolver<BC>>{}, VaryingAlpha<lbman::QTensorSolver<BC>>{});
+    sub("q_init_only", InitOnly<QTensorSolver<BC>>{}, InitOnly<lbman::QTensorSolver<BC>>{});
 }
 
 }  // namespace

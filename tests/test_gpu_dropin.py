@@ -11,7 +11,15 @@ anchoring / moving-wall box of 10x12x8 cells:
   * lbman::LbmSolver<BC> (src/lbm_solver.h:12-21) on host fields, populations
     included;
   * lbman::QTensorSolver<BC>::Step (src/qtensor_solver.h:51), new Q and the
-    full body force.
+    full body force;
+  * StepAndSetupBodyForce alone: new and previous Q, Sigma, tau and the
+    Ericksen seed;
+  * subclasses written once over either class: an empty
+    SetActiveStressAndComputeBodyForce (pure relaxation,
+    src/qtensor_solver.h:21), an override that calls the base and adds a
+    space-varying active term (src/qtensor_solver.h:11-19), and one that
+    overrides only Initialize -- an override replaces the activity model on
+    the GPU as it does in the reference.
 """
 import json
 import os
@@ -31,6 +39,8 @@ def test_dropin_bitwise(steps):
     lines = [json.loads(x) for x in r.stdout.splitlines() if x.startswith("{")]
     assert r.returncode == 0, r.stdout + r.stderr
     checks = {(x["check"], x["bc"]) for x in lines}
-    assert len(checks) == 4 * 4, lines
+    names = {"sim", "lbm_init", "lbm", "q", "q_setup", "q_zero", "q_varying", "q_init_only"}
+    assert {c for c, _ in checks} == names, lines
+    assert len(checks) == len(names) * 4, lines
     for x in lines:
         assert x["mismatches"] == 0, x
