@@ -138,7 +138,8 @@ def make_sim(workload, precision, device, kernels="auto", tile=None):
     nx, ny, nz, bc, alpha, _ = WORKLOADS[workload]
     p = L.Params(nx=nx, ny=ny, nz=nz, ALPHA=alpha)
     prec = {"fp64": L.Precision.FP64, "fp32": L.Precision.FP32, "fp16": L.Precision.FP16}[precision]
-    kern = {"auto": L._native.KERNELS_AUTO, "split": L._native.KERNELS_SPLIT, "fused": L._native.KERNELS_FUSED}[kernels]
+    kern = {"auto": L._native.KERNELS_AUTO, "split": L._native.KERNELS_SPLIT, "fused": L._native.KERNELS_FUSED,
+            "pair": L._native.KERNELS_SPLIT_PAIR}[kernels]
     sim = L.Simulation(p, bc_for(bc), prec, kern, device=device, tile=tile)
     return sim, p
 
@@ -415,7 +416,7 @@ def main():
     ap.add_argument("--error-steps", type=int, default=2000,
                     help="steps of the FP32/FP16 runs compared with the FP64 path")
     ap.add_argument("--no-extras", action="store_true", help="skip e2e, cpu baseline and variants")
-    ap.add_argument("--kernels", default="auto", choices=["auto", "fused", "split"])
+    ap.add_argument("--kernels", default="auto", choices=["auto", "fused", "split", "pair"])
     ap.add_argument("--tile", default=None, help="tcx,tcy[,zchunk] of the z-marching kernels")
     a = ap.parse_args()
 
@@ -462,7 +463,7 @@ def main():
         tuned = sim.autotune(steps_per_trial=8 if V > 5e7 else 10)
         config["autotuned"] = {k: tuned[k] for k in ("kernels", "tile_x", "tile_y", "zchunk", "trials")}
     sh = sim.shape()
-    config["kernels"] = {1: "split", 2: "fused"}[sh["kernels"]]
+    config["kernels"] = {1: "split", 2: "fused", 3: "split_pair"}[sh["kernels"]]
     config["tile"] = [sh["tile_x"], sh["tile_y"], sh["zchunk"]]
     if world > 1:
         dist.barrier()

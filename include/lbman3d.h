@@ -61,6 +61,10 @@ extern "C" {
 #define LBMAN_KERNELS_AUTO 0
 #define LBMAN_KERNELS_SPLIT 1 /* Q+force kernel, then LBM kernel               */
 #define LBMAN_KERNELS_FUSED 2 /* one kernel per time step                      */
+#define LBMAN_KERNELS_SPLIT_PAIR 3 /* split, the Q+force kernel updating two
+                                 points per thread with packed FP32 pairs
+                                 (FP32/FP16 precision; tiles 32x6, 32x8,
+                                 32x14, 64x6; nx a multiple of 4)            */
 
 /* One face of the box: WallSpec<QBC, UBC> (src/boundary.h:72-76). */
 typedef struct lbman_face {
@@ -206,7 +210,7 @@ int lbman_flow_reduce_noalloc(int64_t ncells, int precision, const void* rho, co
 
 /* Launch shape of the time step: kernel organisation and z-marching tile.   */
 typedef struct lbman_shape {
-    int kernels;              /* LBMAN_KERNELS_SPLIT / LBMAN_KERNELS_FUSED     */
+    int kernels;              /* LBMAN_KERNELS_SPLIT / _FUSED / _SPLIT_PAIR   */
     int tile_x, tile_y;       /* cells per x-y plane of one block             */
     int zchunk;               /* > 0: z planes marched by one block;
                                  <= 0: balanced schedule, max(1, -zchunk)

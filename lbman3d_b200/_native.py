@@ -16,7 +16,7 @@ Q_PERIODIC, Q_NEUMANN, Q_ANCHORING = 0, 1, 2
 U_PERIODIC, U_NOSLIP, U_MOVING, U_SPECULAR = 0, 1, 2, 3
 CENTRED, UPWIND = 0, 1
 FP64, FP32, FP16 = 0, 1, 2
-KERNELS_AUTO, KERNELS_SPLIT, KERNELS_FUSED = 0, 1, 2
+KERNELS_AUTO, KERNELS_SPLIT, KERNELS_FUSED, KERNELS_SPLIT_PAIR = 0, 1, 2, 3
 DIAG_FLOW, DIAG_ENERGY, DIAG_DEFECTS, DIAG_ALL = 1, 2, 4, 7
 
 

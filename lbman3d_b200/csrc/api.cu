@@ -194,9 +194,13 @@ int default_zchunk(int nx, int ny, int nz, int tcx, int tcy, int num_sms) {
 // per output cell (threads per tile cell times the x and y padding).
 LaunchShape default_shape(const lbman_config& c, int num_sms, const Ops& ops) {
     LaunchShape L;
+    L.tile.pair = c.kernels == LBMAN_KERNELS_SPLIT_PAIR;
     if (c.tile_x > 0 && c.tile_y > 0) {
         L.tile.tcx = c.tile_x;
         L.tile.tcy = c.tile_y;
+    } else if (L.tile.pair) {
+        L.tile.tcx = 32;
+        L.tile.tcy = 8;
     } else {
         double best = 1e30;
         int best_wide = -1;
@@ -232,7 +236,9 @@ int validate(const lbman_config& c) {
     if (V >= 2147483648.0) return fail(LBMAN_ERR_UNSUPPORTED, "grids of 2^31 cells or more are not supported");
     if (c.precision < LBMAN_FP64 || c.precision > LBMAN_FP16) return fail(LBMAN_ERR_ARG, "bad precision");
     if (c.advection != LBMAN_CENTRED && c.advection != LBMAN_UPWIND) return fail(LBMAN_ERR_ARG, "bad advection");
-    if (c.kernels < LBMAN_KERNELS_AUTO || c.kernels > LBMAN_KERNELS_FUSED) return fail(LBMAN_ERR_ARG, "bad kernels");
+    if (c.kernels < LBMAN_KERNELS_AUTO || c.kernels > LBMAN_KERNELS_SPLIT_PAIR) return fail(LBMAN_ERR_ARG, "bad kernels");
+    if (c.kernels == LBMAN_KERNELS_SPLIT_PAIR && (c.precision == LBMAN_FP64 || (c.nx & 3) != 0))
+        return fail(LBMAN_ERR_ARG, "LBMAN_KERNELS_SPLIT_PAIR needs FP32 or FP16 precision and nx a multiple of 4");
     if (!(c.TAUF > 0.0) || !(c.DT > 0.0) || !(c.kDensity > 0.0)) return fail(LBMAN_ERR_ARG, "TAUF, DT, kDensity must be > 0");
     for (int k = 0; k < 6; ++k) {
         const lbman_face& f = c.face[k];
@@ -798,12 +804,17 @@ int lbman_get_shape(lbman_solver* s, lbman_shape* out) {
 
 int lbman_set_shape(lbman_solver* s, const lbman_shape* sh) {
     if (!s || !sh) return fail(LBMAN_ERR_ARG, "null argument");
-    if (sh->kernels != LBMAN_KERNELS_SPLIT && sh->kernels != LBMAN_KERNELS_FUSED)
-        return fail(LBMAN_ERR_ARG, "kernels must be LBMAN_KERNELS_SPLIT or LBMAN_KERNELS_FUSED");
+    if (sh->kernels != LBMAN_KERNELS_SPLIT && sh->kernels != LBMAN_KERNELS_FUSED &&
+        sh->kernels != LBMAN_KERNELS_SPLIT_PAIR)
+        return fail(LBMAN_ERR_ARG, "kernels must be LBMAN_KERNELS_SPLIT, LBMAN_KERNELS_FUSED or LBMAN_KERNELS_SPLIT_PAIR");
     QTile t{sh->tile_x, sh->tile_y, sh->zchunk};
+    t.pair = sh->kernels == LBMAN_KERNELS_SPLIT_PAIR;
     if (sh->zchunk < -8) return fail(LBMAN_ERR_ARG, "zchunk must be >= -8 (<= 0: balanced schedule)");
+    if (t.pair && (s->prec == LBMAN_FP64 || (s->P.nx & 3) != 0))
+        return fail(LBMAN_ERR_ARG, "LBMAN_KERNELS_SPLIT_PAIR needs FP32 or FP16 precision and nx a multiple of 4");
     if (s->ops().qforce_smem(t) == 0)
-        return fail(LBMAN_ERR_ARG, "tile %dx%d is not compiled for this precision", sh->tile_x, sh->tile_y);
+        return fail(LBMAN_ERR_ARG, "tile %dx%d is not compiled for this precision%s", sh->tile_x, sh->tile_y,
+                    t.pair ? " and organisation" : "");
     s->kernels = sh->kernels;
     s->shape.tile = t;
     s->shape.qthreads = s->ops().qforce_threads(t);
@@ -843,9 +854,11 @@ int lbman_autotune(lbman_solver* s, int steps_per_trial, lbman_shape* best, int*
     if (copy_state(true) != cudaSuccess || cudaEventCreate(&e0) != cudaSuccess || cudaEventCreate(&e1) != cudaSuccess) {
         status = fail(LBMAN_ERR_CUDA, "autotune set-up failed");
     } else {
-        for (int k : {LBMAN_KERNELS_SPLIT, LBMAN_KERNELS_FUSED}) {
+        for (int k : {LBMAN_KERNELS_SPLIT, LBMAN_KERNELS_FUSED, LBMAN_KERNELS_SPLIT_PAIR}) {
+            if (k == LBMAN_KERNELS_SPLIT_PAIR && (s->prec == LBMAN_FP64 || (s->P.nx & 3) != 0)) continue;
             for (const auto& t : kTileList) {
                 QTile q{t[0], t[1], 1};
+                q.pair = k == LBMAN_KERNELS_SPLIT_PAIR;
                 if (s->ops().qforce_smem(q) == 0) continue;
                 // the balanced one-wave schedule, then fixed chunks around the
                 // default chunk length

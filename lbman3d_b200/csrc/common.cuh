@@ -81,6 +81,7 @@ inline void fill_float_phys(SimParams& P) {
 struct QTile {
     int tcx, tcy;  // output cells per plane
     int zc;        // z planes per block
+    int pair = 0;  // FP32 Q+force kernel with two points per thread (qpair.cuh)
 };
 
 // D3Q15 (src/lattice_stencil.h:42-76): velocities, weights, opposite and

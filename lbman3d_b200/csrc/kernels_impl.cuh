@@ -5,6 +5,7 @@
 #include "fused.cuh"
 #include "init.cuh"
 #include "qsplit.cuh"
+#include "qpair.cuh"
 #include "launch.h"
 #include "reduce.cuh"
 #include "tiles.h"
@@ -42,10 +43,34 @@ cudaError_t with_tile(int tcx, int tcy, F&& f) {
     return cudaErrorInvalidValue;
 }
 
+// Calls f(PairTile<...>{}) for a compiled pair tile (FP32 compute only);
+// cudaErrorInvalidValue for any other shape or precision.
+template <class R, class F>
+cudaError_t with_pair_tile(int tcx, int tcy, F&& f) {
+    if constexpr (sizeof(R) == 4) {
+#define LBMAN_TILE(X, Y)                                                       \
+    if (tcx == X && tcy == Y) {                                                \
+        if constexpr (PairTile<X, Y>::template smem_bytes<R>() <= kMaxSmem)    \
+            return f(PairTile<X, Y>{});                                        \
+        else                                                                   \
+            return cudaErrorInvalidValue;                                      \
+    }
+        LBMAN_PAIR_TILES(LBMAN_TILE)
+#undef LBMAN_TILE
+    }
+    return cudaErrorInvalidValue;
+}
+
+// with_tile or with_pair_tile, as the shape says
+template <class R, class F>
+cudaError_t with_qtile(const QTile& T, F&& f) {
+    return T.pair ? with_pair_tile<R>(T.tcx, T.tcy, f) : with_tile<R>(T.tcx, T.tcy, f);
+}
+
 template <class R>
 size_t qforce_smem(const QTile& T) {
     size_t b = 0;
-    with_tile<R>(T.tcx, T.tcy, [&](auto tl) {
+    with_qtile<R>(T, [&](auto tl) {
         b = decltype(tl)::template smem_bytes<R>();
         return cudaSuccess;
     });
@@ -55,7 +80,7 @@ size_t qforce_smem(const QTile& T) {
 template <class R>
 int qforce_threads(const QTile& T) {
     int n = 0;
-    with_tile<R>(T.tcx, T.tcy, [&](auto tl) {
+    with_qtile<R>(T, [&](auto tl) {
         n = decltype(tl)::NT;
         return cudaSuccess;
     });
@@ -90,9 +115,37 @@ dim3 march_grid(const SimParams& P, const LaunchShape& S, size_t smem) {
     return dim3((unsigned)std::max<int64_t>(1, std::min(units, grid)));
 }
 
+// The pair kernel stages 16-byte chunks: nx a multiple of 4 and 16-byte
+// aligned fields (every field offset k V is then a multiple of 4 floats).
+inline bool pair_ok(const SimParams& P, const void* qin, const void* uin) {
+    return (P.nx & 3) == 0 && ((reinterpret_cast<uintptr_t>(qin) | reinterpret_cast<uintptr_t>(uin)) & 15) == 0;
+}
+
 template <class R>
 cudaError_t qforce(const SimParams& P, const LaunchShape& S, const void* qin, const void* uin, void* qout,
                    void* Fout, cudaStream_t st) {
+    if (S.tile.pair) {
+        if constexpr (sizeof(R) == 4) {
+            if (!pair_ok(P, qin, uin)) return cudaErrorInvalidValue;
+            return with_pair_tile<R>(S.tile.tcx, S.tile.tcy, [&](auto tl) {
+                using TL = decltype(tl);
+                const size_t smem = TL::template smem_bytes<R>();
+                if (P.upwind) {
+                    constexpr auto K = qpair_kernel<TL, true>;
+                    K<<<march_grid<TL, K>(P, S, smem), TL::NT, smem, st>>>(P, S.tile.zc, (const float*)qin,
+                                                                           (const float*)uin, (float*)qout,
+                                                                           (float*)Fout);
+                } else {
+                    constexpr auto K = qpair_kernel<TL, false>;
+                    K<<<march_grid<TL, K>(P, S, smem), TL::NT, smem, st>>>(P, S.tile.zc, (const float*)qin,
+                                                                           (const float*)uin, (float*)qout,
+                                                                           (float*)Fout);
+                }
+                return cudaGetLastError();
+            });
+        }
+        return cudaErrorInvalidValue;
+    }
     return with_tile<R>(S.tile.tcx, S.tile.tcy, [&](auto tl) {
         using TL = decltype(tl);
         const size_t smem = TL::template smem_bytes<R>();
@@ -135,6 +188,19 @@ cudaError_t fused(const SimParams& P, const LaunchShape& L, bool first, const vo
 template <class R, class S, bool DEV>
 int march_blocks(const SimParams& P, const LaunchShape& L, bool fused_org) {
     int n = 0;
+    if (L.tile.pair) {
+        if constexpr (sizeof(R) == 4) {
+            with_pair_tile<R>(L.tile.tcx, L.tile.tcy, [&](auto tl) {
+                using TL = decltype(tl);
+                const size_t smem = TL::template smem_bytes<R>();
+                const dim3 g = P.upwind ? march_grid<TL, qpair_kernel<TL, true>>(P, L, smem)
+                                        : march_grid<TL, qpair_kernel<TL, false>>(P, L, smem);
+                n = (int)(g.x * g.y * g.z);
+                return cudaSuccess;
+            });
+        }
+        return n;
+    }
     with_tile<R>(L.tile.tcx, L.tile.tcy, [&](auto tl) {
         using TL = decltype(tl);
         const size_t smem = TL::template smem_bytes<R>();
@@ -307,6 +373,16 @@ cudaError_t prepare(size_t max_smem) {
             attr(fused_kernel<TL, R, S, DEV, false>);
             return cudaSuccess;
         });
+    }
+    if constexpr (sizeof(R) == 4) {
+        for (const auto& xy : kPairTileList) {
+            with_pair_tile<R>(xy[0], xy[1], [&](auto tl) {
+                using TL = decltype(tl);
+                attr(qpair_kernel<TL, true>);
+                attr(qpair_kernel<TL, false>);
+                return cudaSuccess;
+            });
+        }
     }
     return e;
 }

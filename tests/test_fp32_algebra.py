@@ -32,3 +32,16 @@ def test_fp32_paired_relaxation_matches_reference_form(tmp_path):
                     os.path.join(HERE, "host", "collide_check.cpp"), "-o", exe], check=True)
     r = subprocess.run([exe], capture_output=True, text=True)
     assert r.returncode == 0, r.stdout + r.stderr
+
+
+@pytest.mark.skipif(shutil.which("g++") is None, reason="needs g++")
+def test_packed_pair_rhs_matches_reference_form(tmp_path):
+    """The two-point packed FP32 right-hand side (csrc/physics_pair.cuh
+    pointwise_q_pair: Q_new, row stress, Ericksen force) against the
+    reference-ordered pointwise_q in double, per point, centred and upwind;
+    FP32 rounding only."""
+    exe = str(tmp_path / "pair_check")
+    subprocess.run(["g++", "-std=c++17", "-O1", "-I", os.path.join(HERE, "host", "stub"), "-I", CSRC,
+                    os.path.join(HERE, "host", "pair_check.cpp"), "-o", exe], check=True)
+    r = subprocess.run([exe], capture_output=True, text=True)
+    assert r.returncode == 0, r.stdout + r.stderr
