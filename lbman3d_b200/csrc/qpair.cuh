@@ -345,13 +345,16 @@ __device__ __forceinline__ void qp_march(const SimParams& P, int x0, int y0, int
     cp_async_wait_all();
     __syncthreads();
     const int rm = (G.wx || G.wy || G.wz) ? ((G.wy || G.wz) ? 2 : 1) : 0;
-    auto compute = [&](int zb, F2 er[3], F2 qn[5], F2 u[3]) {
-        if (rm == 0) qp_compute_plane<TL, UPWIND, 0>(P, K, G, R, z0, zb, QU, Bs, er, qn, u);
-        else if (rm == 1) qp_compute_plane<TL, UPWIND, 1>(P, K, G, R, z0, zb, QU, Bs, er, qn, u);
-        else qp_compute_plane<TL, UPWIND, 2>(P, K, G, R, z0, zb, QU, Bs, er, qn, u);
-    };
-    compute(z0 - 1, er_next, qn_next, u_next);
-    compute(z0, er_cur, qn_cur, u_cur);
+    // (a macro, not a lambda: passing the pair arrays to a lambda put them in
+    // local memory)
+#define LBMAN_QP_COMPUTE(zb, er, qn, u)                                                      \
+    do {                                                                                    \
+        if (rm == 0) qp_compute_plane<TL, UPWIND, 0>(P, K, G, R, z0, zb, QU, Bs, er, qn, u); \
+        else if (rm == 1) qp_compute_plane<TL, UPWIND, 1>(P, K, G, R, z0, zb, QU, Bs, er, qn, u); \
+        else qp_compute_plane<TL, UPWIND, 2>(P, K, G, R, z0, zb, QU, Bs, er, qn, u);         \
+    } while (0)
+    LBMAN_QP_COMPUTE(z0 - 1, er_next, qn_next, u_next);
+    LBMAN_QP_COMPUTE(z0, er_cur, qn_cur, u_cur);
     __syncthreads();  // the slot of z0-2 is free again
     qf_load_plane<TL>(P, x0, y0, z0, z0 + 2, qin, uin, QU, true, ps);
     cp_async_wait_all();
@@ -359,7 +362,7 @@ __device__ __forceinline__ void qp_march(const SimParams& P, int x0, int y0, int
 #pragma unroll 1
     for (int zc = z0; zc < z1; ++zc) {
         if (zc + 1 < z1) qf_load_plane<TL>(P, x0, y0, z0, zc + 3, qin, uin, QU, true, ps);
-        compute(zc + 1, er_next, qn_next, u_next);
+        LBMAN_QP_COMPUTE(zc + 1, er_next, qn_next, u_next);
         // no barrier here: the force of plane zc reads results of plane zc
         // written before the last barrier, in slots plane zc + 1 does not use
         if (rm == 0) qp_force<TL, 0>(P, K, G, R, x0, y0, z0, zc, Bs, er_cur, qn_cur, u_cur, out);
@@ -375,6 +378,7 @@ __device__ __forceinline__ void qp_march(const SimParams& P, int x0, int y0, int
         cp_async_wait_all();
         __syncthreads();
     }
+#undef LBMAN_QP_COMPUTE
 }
 
 // Consumer of the split organisation: Q_new and the body force of one cell.
