@@ -63,8 +63,8 @@ extern "C" {
 #define LBMAN_KERNELS_FUSED 2 /* one kernel per time step                      */
 #define LBMAN_KERNELS_SPLIT_PAIR 3 /* split, the Q+force kernel updating two
                                  points per thread with packed FP32 pairs
-                                 (FP32/FP16 precision; tiles 32x6, 32x8,
-                                 32x14, 64x6; nx a multiple of 4)            */
+                                 (FP32/FP16 precision; tiles 30x6, 30x10,
+                                 30x14; nx a multiple of 4)                  */
 
 /* One face of the box: WallSpec<QBC, UBC> (src/boundary.h:72-76). */
 typedef struct lbman_face {

@@ -199,8 +199,8 @@ LaunchShape default_shape(const lbman_config& c, int num_sms, const Ops& ops) {
         L.tile.tcx = c.tile_x;
         L.tile.tcy = c.tile_y;
     } else if (L.tile.pair) {
-        L.tile.tcx = 32;
-        L.tile.tcy = 8;
+        L.tile.tcx = 30;
+        L.tile.tcy = 10;
     } else {
         double best = 1e30;
         int best_wide = -1;
@@ -863,9 +863,14 @@ int lbman_autotune(lbman_solver* s, int steps_per_trial, lbman_shape* best, int*
                 // the balanced one-wave schedule, then fixed chunks around the
                 // default chunk length
                 const int z0 = default_zchunk(s->P.nx, s->P.ny, s->P.nz, t[0], t[1], s->num_sms);
-                int zs[6] = {0, -2, -3, z0, std::max(4, z0 / 2), std::min(s->P.nz, 2 * z0)};
-                for (int zi = 0; zi < 6 && status == LBMAN_OK; ++zi) {
-                    if (zi > 3 && (zs[zi] == z0 || (zi == 5 && zs[5] == zs[4]))) continue;
+                // plus 32- and 64-plane chunks: many waves of medium marches keep
+                // the blocks of an SM out of step (measured best for the pair
+                // kernel on large boxes)
+                int zs[8] = {0, -2, -3, z0, std::max(4, z0 / 2), std::min(s->P.nz, 2 * z0), 32, 64};
+                for (int zi = 0; zi < 8 && status == LBMAN_OK; ++zi) {
+                    bool seen = false;
+                    for (int zj = 0; zj < zi; ++zj) seen = seen || zs[zj] == zs[zi];
+                    if (seen || (zi >= 6 && zs[zi] >= s->P.nz)) continue;
                     cur = {k, t[0], t[1], zs[zi], 0, 0.0};
                     if (lbman_set_shape(s, &cur) != LBMAN_OK) continue;
                     if ((status = one_step(s, false)) != LBMAN_OK) break;

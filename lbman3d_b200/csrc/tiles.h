@@ -5,7 +5,7 @@
 
 #define LBMAN_TILES(X) X(30, 6) X(32, 6) X(14, 14) X(30, 14) X(62, 6) X(32, 8) X(32, 14) X(64, 6)
 // tiles of the two-points-per-thread FP32 Q+force kernel (qpair.cuh)
-#define LBMAN_PAIR_TILES(X) X(32, 6) X(32, 8) X(32, 14) X(64, 6)
+#define LBMAN_PAIR_TILES(X) X(30, 6) X(30, 10) X(30, 14)
 
 namespace lbman {
 #define LBMAN_TILE_PAIR(x, y) {x, y},

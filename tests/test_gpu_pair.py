@@ -43,7 +43,8 @@ def _sim(grid, faces, phys, upwind, precision=L.Precision.FP32, kernels=PAIR, ti
     return L.Simulation(p, L.from_face_tuples(faces), precision, kernels, tile=tile)
 
 
-# nx a multiple of 4 (16-byte staging); 36 and 44 leave partial 32-wide tiles
+# nx a multiple of 4 (16-byte staging); none is a multiple of 30, so every
+# box has a partial tile in x
 CASES = [
     ("periodic", (64, 20, 16), False),
     ("channel", (32, 26, 12), False),
@@ -54,7 +55,7 @@ CASES = [
     ("walls", (40, 10, 9), False),
     ("anchored_z", (32, 12, 11), False),
 ]
-TILES = [(32, 6, 0), (32, 8, 5), (32, 14, 0), (64, 6, 4)]
+TILES = [(30, 6, 0), (30, 10, 5), (30, 14, 0), (30, 10, 3)]
 
 
 @pytest.mark.parametrize("tile", TILES, ids=[f"{t[0]}x{t[1]}z{t[2]}" for t in TILES])
@@ -84,7 +85,7 @@ def test_pair_kernel_vs_one_point_kernel(bc, grid, upwind):
     phys = dict(ALPHA=0.01)
     _, rho, u, q = _case(grid, BC[bc], upwind, **phys)
     outs = []
-    for kernels, tile in ((L._native.KERNELS_SPLIT, (32, 8, 0)), (PAIR, (32, 8, 0))):
+    for kernels, tile in ((L._native.KERNELS_SPLIT, (32, 8, 0)), (PAIR, (30, 10, 0))):
         sim = _sim(grid, BC[bc], phys, upwind, kernels=kernels, tile=tile)
         sim.upload(rho, u, q)
         sim.qtensor_step()
@@ -102,7 +103,7 @@ def test_pair_kernel_fp16_storage_vs_fp64_oracle(bc):
     p, rho, u, q = _case(grid, BC[bc], False, ALPHA=0.01)
     ref = O.OracleSim(p)
     ref.set(rho, u, q)
-    sim = _sim(grid, BC[bc], dict(ALPHA=0.01), False, precision=L.Precision.FP16, tile=(32, 8, 0))
+    sim = _sim(grid, BC[bc], dict(ALPHA=0.01), False, precision=L.Precision.FP16, tile=(30, 10, 0))
     sim.upload(rho, u, q)
     for n, tol in ((1, 1e-3), (19, 1e-2)):
         ref.step(n)
@@ -116,6 +117,6 @@ def test_pair_kernel_fp16_storage_vs_fp64_oracle(bc):
 def test_pair_organisation_rejected_where_it_cannot_run():
     from cases import BC
     with pytest.raises(L._native.LbmanError):  # FP64 keeps the reference's arithmetic
-        _sim((32, 8, 8), BC["periodic"], {}, False, precision=L.Precision.FP64, tile=(32, 8, 0))
+        _sim((32, 8, 8), BC["periodic"], {}, False, precision=L.Precision.FP64, tile=(30, 10, 0))
     with pytest.raises(L._native.LbmanError):  # nx not a multiple of 4
-        _sim((30, 8, 8), BC["periodic"], {}, False, tile=(32, 8, 0))
+        _sim((30, 8, 8), BC["periodic"], {}, False, tile=(30, 10, 0))
