@@ -51,6 +51,9 @@ struct Ops {
     decltype(&launch_fused_f64) fused;
     decltype(&launch_lbm_f64) lbm;
     decltype(&launch_stream_only_f64) stream_only;
+    decltype(&launch_lbm_aa_f64) lbm_aa;
+    decltype(&launch_aa_pop_out_f64) aa_pop_out;
+    decltype(&launch_swap_pairs_f64) swap_pairs;
     decltype(&launch_feq_init_f64) feq_init;
     decltype(&launch_pop_in_f64) pop_in;
     decltype(&launch_pop_out_f64) pop_out;
@@ -73,6 +76,7 @@ struct Ops {
 #define LBMAN_OPS(SUF)                                                                                 \
     Ops {                                                                                              \
         launch_qforce_##SUF, launch_fused_##SUF, launch_lbm_##SUF, launch_stream_only_##SUF,           \
+            launch_lbm_aa_##SUF, launch_aa_pop_out_##SUF, launch_swap_pairs_##SUF,                     \
             launch_feq_init_##SUF, launch_pop_in_##SUF, launch_pop_out_##SUF, launch_real_in_##SUF,    \
             launch_real_out_##SUF, launch_flow_reduce_##SUF, launch_energy_reduce_##SUF,               \
             launch_director_##SUF, launch_defect_count_##SUF, launch_defect_flags_##SUF,              \
@@ -134,6 +138,8 @@ void build_sim_params(const lbman_config& c, SimParams& P) {
 }
 }  // namespace lbman
 
+enum { F_PRE = 0, F_POST = 1, F_SWAP = 2 };
+
 struct lbman_solver {
     lbman_config cfg;
     SimParams P;
@@ -156,7 +162,13 @@ struct lbman_solver {
     void* upast = nullptr;
     void* dirbuf = nullptr;
     int fcur = 0, qcur = 0, ucur = 0;
-    bool uploaded = false, f_post = false;
+    // Layout of the populations in f[fcur]: F_PRE pre-collision (after an
+    // upload or an odd in-place step), F_POST post-collision of the
+    // two-buffer kernels (fused organisation), F_SWAP post-collision in the
+    // in-place layout (after an even in-place step).  f[1] exists only once
+    // the fused organisation has run.
+    int fphase = 0;
+    bool uploaded = false;
     cudaStream_t stream = nullptr;
     bool own_stream = false;
     int64_t steps = 0, launches = 0;
@@ -384,15 +396,17 @@ int lbman_create(const lbman_config* cfg, lbman_solver** out) {
         if (e != cudaSuccess) return fail(LBMAN_ERR_NOMEM, "cudaMalloc(%zu) failed: %s", bytes, cudaGetErrorString(e));
         return LBMAN_OK;
     };
+    // one population buffer: the split organisations stream in place
+    if (int st = alloc(&s->f[0], 15 * V * s->sbytes)) return bail(st);
     for (int b = 0; b < 2; ++b) {
-        if (int st = alloc(&s->f[b], 15 * V * s->sbytes)) return bail(st);
         if (int st = alloc(&s->q[b], 5 * V * s->rbytes)) return bail(st);
         if (int st = alloc(&s->u[b], 3 * V * s->rbytes)) return bail(st);
     }
     if (int st = alloc(&s->rho, V * s->rbytes)) return bail(st);
     if (int st = alloc(&s->F, 3 * V * s->rbytes)) return bail(st);
-    if (s->prec != LBMAN_FP64)
-        if (int st = alloc((void**)&s->staging, V * sizeof(double))) return bail(st);
+    // FP64 host staging too: downloads of an in-place-layout state gather
+    // into it
+    if (int st = alloc((void**)&s->staging, V * sizeof(double))) return bail(st);
     s->red_G = (int)std::min<int64_t>((V + 255) / 256, (int64_t)s->num_sms * 8);
     if (int st = alloc((void**)&s->partials, (size_t)s->red_G * 8 * sizeof(double))) return bail(st);
     if (int st = alloc((void**)&s->red_dev, 16 * sizeof(double))) return bail(st);
@@ -463,7 +477,7 @@ int lbman_upload(lbman_solver* s, const double* rho, const double* u3, const dou
     }
     LB_CUDA(cudaStreamSynchronize(s->stream));
     s->uploaded = true;
-    s->f_post = false;
+    s->fphase = F_PRE;
     s->steps = 0;
     return LBMAN_OK;
 }
@@ -492,7 +506,7 @@ int solver_reset_populations(lbman_solver* s) {
     if (!s->uploaded) return fail(LBMAN_ERR_STATE, "no state to rebuild populations from");
     LB_TRY(set_device(s));
     LB_TRY(check_launch(s, s->ops().feq_init(s->P, s->rho, s->u[s->ucur], s->f[s->fcur], s->stream), "feq_init"));
-    s->f_post = false;
+    s->fphase = F_PRE;
     return LBMAN_OK;
 }
 
@@ -521,7 +535,7 @@ int lbman_init_seeded(lbman_solver* s, uint64_t seed, double S0, double sigma) {
     LB_TRY(check_launch(s, s->ops().feq_init(s->P, s->rho, s->u[s->ucur], s->f[s->fcur], s->stream), "feq_init"));
     LB_CUDA(cudaStreamSynchronize(s->stream));
     s->uploaded = true;
-    s->f_post = false;
+    s->fphase = F_PRE;
     s->steps = 0;
     return LBMAN_OK;
 }
@@ -537,12 +551,16 @@ int lbman_download(lbman_solver* s, double* rho, double* u3, double* q5, double*
     if (force3) for (int k = 0; k < 3; ++k) LB_TRY(stage_out_real(s, vptr(s->F, k * V, s->rbytes), force3 + k * V, V));
     if (f15) {
         const void* src = s->f[s->fcur];
-        if (s->f_post) {  // stream the stored f* into the spare buffer
+        if (s->fphase == F_POST) {  // stream the stored f* into the spare buffer
             LB_TRY(check_launch(s, s->ops().stream_only(s->P, s->f[s->fcur], s->f[1 - s->fcur], s->rho, s->stream), "stream_only"));
             src = s->f[1 - s->fcur];
         }
         for (int j = 0; j < 15; ++j) {
-            if (s->prec == LBMAN_FP64) {
+            if (s->fphase == F_SWAP) {  // the odd step's gather of direction j
+                if (!s->staging) return fail(LBMAN_ERR_STATE, "no staging buffer");
+                LB_TRY(check_launch(s, s->ops().aa_pop_out(s->P, src, s->rho, s->staging, j, s->stream), "aa_pop_out"));
+                LB_CUDA(cudaMemcpyAsync(f15 + j * V, s->staging, V * 8, cudaMemcpyDeviceToHost, s->stream));
+            } else if (s->prec == LBMAN_FP64) {
                 LB_CUDA(cudaMemcpyAsync(f15 + j * V, vptr((void*)src, j * V, 8), V * 8, cudaMemcpyDeviceToHost, s->stream));
             } else {
                 LB_TRY(check_launch(s, s->ops().pop_out(s->P, src, s->staging, j, s->stream), "pop_out"));
@@ -554,10 +572,43 @@ int lbman_download(lbman_solver* s, double* rho, double* u3, double* q5, double*
     return LBMAN_OK;
 }
 
+// The second population buffer of the fused (two-buffer) organisation.
+static int ensure_f1(lbman_solver* s) {
+    if (!s->f[1]) {
+        cudaError_t e = cudaMalloc(&s->f[1], 15 * s->P.V * s->sbytes);
+        if (e != cudaSuccess) {
+            cudaGetLastError();
+            s->f[1] = nullptr;
+            return fail(LBMAN_ERR_NOMEM, "cudaMalloc of the second population buffer failed: %s", cudaGetErrorString(e));
+        }
+    }
+    // the buffers alternate; f[fcur] must be the one in use
+    return LBMAN_OK;
+}
+
+// In-place LBM step (AA pattern): even from F_PRE, odd from F_SWAP; a
+// two-buffer post-collision state is first put in the in-place layout.
+static int aa_step(lbman_solver* s, bool last) {
+    const Ops& o = s->ops();
+    if (s->fphase == F_POST) {
+        LB_TRY(check_launch(s, o.swap_pairs(s->P, s->f[s->fcur], s->stream), "swap_pairs"));
+        s->fphase = F_SWAP;
+    }
+    const bool odd = s->fphase == F_SWAP;
+    LB_TRY(check_launch(s, o.lbm_aa(s->P, odd, last, s->f[s->fcur], s->F, s->rho, s->u[s->ucur], s->stream), "lbm_aa"));
+    s->fphase = odd ? F_PRE : F_SWAP;
+    return LBMAN_OK;
+}
+
 static int one_step(lbman_solver* s, bool last) {
-    const bool first = !s->f_post;
     const Ops& o = s->ops();
     if (s->kernels == LBMAN_KERNELS_FUSED) {
+        LB_TRY(ensure_f1(s));
+        if (s->fphase == F_SWAP) {  // back to the two-buffer layout
+            LB_TRY(check_launch(s, o.swap_pairs(s->P, s->f[s->fcur], s->stream), "swap_pairs"));
+            s->fphase = F_POST;
+        }
+        const bool first = s->fphase == F_PRE;
         LB_TRY(check_launch(s,
                             o.fused(s->P, s->shape, first, s->q[s->qcur], s->u[s->ucur], s->q[1 - s->qcur],
                                     s->u[1 - s->ucur], s->f[s->fcur], s->f[1 - s->fcur], s->rho,
@@ -566,15 +617,13 @@ static int one_step(lbman_solver* s, bool last) {
         s->qcur ^= 1;
         s->ucur ^= 1;
         s->fcur ^= 1;
+        s->fphase = F_POST;
     } else {
         LB_TRY(check_launch(s, o.qforce(s->P, s->shape, s->q[s->qcur], s->u[s->ucur], s->q[1 - s->qcur], s->F, s->stream),
                             "qforce"));
         s->qcur ^= 1;
-        LB_TRY(check_launch(s, o.lbm(s->P, first, last, s->f[s->fcur], s->f[1 - s->fcur], s->F, s->rho, s->u[s->ucur], s->stream),
-                            "lbm"));
-        s->fcur ^= 1;
+        LB_TRY(aa_step(s, last));
     }
-    s->f_post = true;
     ++s->steps;
     return LBMAN_OK;
 }
@@ -653,10 +702,7 @@ int lbman_lbm_step(lbman_solver* s) {
     if (!s) return fail(LBMAN_ERR_ARG, "null solver");
     if (!s->uploaded) return fail(LBMAN_ERR_STATE, "step before upload");
     LB_TRY(set_device(s));
-    LB_TRY(check_launch(s, s->ops().lbm(s->P, !s->f_post, true, s->f[s->fcur], s->f[1 - s->fcur], s->F, s->rho, s->u[s->ucur], s->stream),
-                        "lbm"));
-    s->fcur ^= 1;
-    s->f_post = true;
+    LB_TRY(aa_step(s, true));
     return LBMAN_OK;
 }
 
@@ -832,7 +878,7 @@ int lbman_autotune(lbman_solver* s, int steps_per_trial, lbman_shape* best, int*
     char* snap = nullptr;
     LB_CUDA(cudaMalloc(&snap, fb + qb + ub + rb + ub));
     const int fc = s->fcur, qc = s->qcur, uc = s->ucur;
-    const bool fpost = s->f_post;
+    const int fphase = s->fphase;
     const int64_t steps0 = s->steps;
     auto copy_state = [&](bool save) -> cudaError_t {
         void* dst[5] = {snap, snap + fb, snap + fb + qb, snap + fb + qb + ub, snap + fb + qb + ub + rb};
@@ -856,6 +902,9 @@ int lbman_autotune(lbman_solver* s, int steps_per_trial, lbman_shape* best, int*
     } else {
         for (int k : {LBMAN_KERNELS_SPLIT, LBMAN_KERNELS_FUSED, LBMAN_KERNELS_SPLIT_PAIR}) {
             if (k == LBMAN_KERNELS_SPLIT_PAIR && (s->prec == LBMAN_FP64 || (s->P.nx & 3) != 0)) continue;
+            // the fused organisation needs a second population buffer; a box
+            // too large for it is tuned over the in-place organisations only
+            if (k == LBMAN_KERNELS_FUSED && ensure_f1(s) != LBMAN_OK) continue;
             for (const auto& t : kTileList) {
                 QTile q{t[0], t[1], 1};
                 q.pair = k == LBMAN_KERNELS_SPLIT_PAIR;
@@ -894,7 +943,7 @@ int lbman_autotune(lbman_solver* s, int steps_per_trial, lbman_shape* best, int*
     // Restore the state and the indices it lived in, then adopt the winner.
     if (copy_state(false) != cudaSuccess && status == LBMAN_OK) status = fail(LBMAN_ERR_CUDA, "state restore failed");
     cudaStreamSynchronize(s->stream);
-    s->fcur = fc; s->qcur = qc; s->ucur = uc; s->f_post = fpost; s->steps = steps0;
+    s->fcur = fc; s->qcur = qc; s->ucur = uc; s->fphase = fphase; s->steps = steps0;
     if (e0) cudaEventDestroy(e0);
     if (e1) cudaEventDestroy(e1);
     cudaFree(snap);

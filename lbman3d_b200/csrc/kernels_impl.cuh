@@ -242,6 +242,47 @@ cudaError_t lbm(const SimParams& P, bool first, bool wr, const void* fin, void* 
     return cudaGetLastError();
 }
 
+// One in-place (AA) LBM step: even (PRE -> SWAP) or odd (SWAP -> PRE).
+template <class R, class S, bool DEV>
+cudaError_t lbm_aa(const SimParams& P, bool odd, bool wr, void* f, const void* F, void* rho, void* uout,
+                   cudaStream_t st) {
+    const FastDiv dnx = make_fastdiv((uint32_t)P.nx), dnxy = make_fastdiv((uint32_t)P.nxy);
+    const unsigned nb = blocks_for(P.V, 256);
+    auto launch = [&](auto kern) {
+        kern<<<nb, 256, 0, st>>>(P, dnx, dnxy, (S*)f, (const R*)F, (R*)rho, (R*)uout, wr ? 1 : 0);
+    };
+    const bool walls = !(P.uper[0] && P.uper[2] && P.uper[4]);
+    const bool i32 = 15 * P.V < ((int64_t)1 << 31);
+#define LBMAN_AA(W, I)                                                        \
+    do {                                                                      \
+        if (odd) launch(lbm_aa_odd_kernel<R, S, DEV, W, I>);                  \
+        else launch(lbm_aa_even_kernel<R, S, DEV, W, I>);                     \
+    } while (0)
+    if (walls) {
+        if (i32) LBMAN_AA(true, int);
+        else LBMAN_AA(true, int64_t);
+    } else {
+        if (i32) LBMAN_AA(false, int);
+        else LBMAN_AA(false, int64_t);
+    }
+#undef LBMAN_AA
+    return cudaGetLastError();
+}
+
+template <class R, class S, bool DEV>
+cudaError_t aa_pop_out(const SimParams& P, const void* f, const void* rho, double* dst, int dir, cudaStream_t st) {
+    const FastDiv dnx = make_fastdiv((uint32_t)P.nx), dnxy = make_fastdiv((uint32_t)P.nxy);
+    aa_pop_out_kernel<R, S, DEV><<<blocks_for(P.V, 256), 256, 0, st>>>(P, dnx, dnxy, (const S*)f, (const R*)rho, dst,
+                                                                      dir);
+    return cudaGetLastError();
+}
+
+template <class S>
+cudaError_t swap_pairs(const SimParams& P, void* f, cudaStream_t st) {
+    swap_pairs_kernel<S><<<blocks_for(P.V, 256), 256, 0, st>>>(P.V, (S*)f);
+    return cudaGetLastError();
+}
+
 template <class R, class S>
 cudaError_t stream_only(const SimParams& P, const void* fin, void* fout, const void* rho, cudaStream_t st) {
     const FastDiv dnx = make_fastdiv((uint32_t)P.nx), dnxy = make_fastdiv((uint32_t)P.nxy);
@@ -411,6 +452,17 @@ cudaError_t prepare(size_t max_smem) {
     cudaError_t launch_stream_only_##SUF(const SimParams& P, const void* fin, void* fout,              \
                                          const void* rho, cudaStream_t st) {                           \
         return impl::stream_only<R, S>(P, fin, fout, rho, st);                                          \
+    }                                                                                                   \
+    cudaError_t launch_lbm_aa_##SUF(const SimParams& P, bool odd, bool wr, void* f, const void* F,     \
+                                    void* rho, void* uout, cudaStream_t st) {                          \
+        return impl::lbm_aa<R, S, DEV>(P, odd, wr, f, F, rho, uout, st);                                \
+    }                                                                                                   \
+    cudaError_t launch_aa_pop_out_##SUF(const SimParams& P, const void* f, const void* rho, double* dst, \
+                                        int dir, cudaStream_t st) {                                    \
+        return impl::aa_pop_out<R, S, DEV>(P, f, rho, dst, dir, st);                                    \
+    }                                                                                                   \
+    cudaError_t launch_swap_pairs_##SUF(const SimParams& P, void* f, cudaStream_t st) {                \
+        return impl::swap_pairs<S>(P, f, st);                                                           \
     }                                                                                                   \
     cudaError_t launch_feq_init_##SUF(const SimParams& P, const void* rho, const void* u, void* f,     \
                                       cudaStream_t st) {                                               \

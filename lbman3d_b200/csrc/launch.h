@@ -30,6 +30,11 @@ struct LaunchShape {
                                  void* fout, const void* F, void* rho, void* uout, cudaStream_t st);   \
     cudaError_t launch_stream_only_##SUF(const SimParams& P, const void* fin, void* fout,              \
                                          const void* rho, cudaStream_t st);                            \
+    cudaError_t launch_lbm_aa_##SUF(const SimParams& P, bool odd, bool write_rho_all, void* f,         \
+                                    const void* F, void* rho, void* uout, cudaStream_t st);            \
+    cudaError_t launch_aa_pop_out_##SUF(const SimParams& P, const void* f, const void* rho, double* dst, \
+                                        int dir, cudaStream_t st);                                     \
+    cudaError_t launch_swap_pairs_##SUF(const SimParams& P, void* f, cudaStream_t st);                 \
     cudaError_t launch_feq_init_##SUF(const SimParams& P, const void* rho, const void* u, void* f,     \
                                       cudaStream_t st);                                                \
     cudaError_t launch_pop_in_##SUF(const SimParams& P, const double* src, void* dst, int dir,         \

@@ -311,6 +311,258 @@ __global__ void __launch_bounds__(256, lbm_min_blocks<R, S, WALLS>()) lbm_kernel
     if (write_rho_all || mv) rho_buf[c] = rho;
 }
 
+// ---- in-place streaming (AA pattern), one population buffer ---------------
+//
+// The buffer alternates between two layouts:
+//   PRE  : F[i][c] = pre-collision f_i(c) (what an upload leaves, and what
+//          the reference stores);
+//   SWAP : F[opp(i)][c] = post-collision f*_i(c).
+// Even step (PRE -> SWAP): each cell reads its own 15 slots, collides and
+// writes f*_i into its own slot opp(i).
+// Odd step (SWAP -> PRE): each cell gathers f_j(c) = f*_j(c - e_j) from slot
+// opp(j) of cell c - e_j (periodic axes wrap), or, when c - e_j lies beyond
+// a wall, from its own slot opp(bi) holding f*_bi(c) (bi: the source the
+// reference's wall rules leave in slot j, as in gather() above; a moving
+// wall adds 6 rho w_j (e_j . U) with rho of the even step); it collides and
+// scatters: f*_k to slot k of cell c + e_k, or, when c + e_k lies beyond a
+// wall, f*_bi(opp k) (+ the moving-wall term with this step's rho) to its own
+// slot opp(k) -- the pre-collision value the next even step reads there.
+// Every slot is read and written by one thread only (the slot (k, x) of an
+// odd step by cell x - e_k; a wall cell's own wall slots by itself), so one
+// buffer serves both steps; the gathered values and the collision are those
+// of the two-buffer kernel, bit for bit.
+
+// Source of slot j of a wall cell: per crossed axis A the candidate opp(j)
+// (no-slip / moving) or spec_A(j) (specular), the largest winning.  Also
+// returns slot = opp(bi), where a SWAP-layout buffer holds f*_bi of the cell
+// (chosen among compile-time candidates, so no table is indexed at run time).
+__device__ __forceinline__ int wall_bi(const SimParams& P, int j, bool cx, bool cy, bool cz, int& slot) {
+    const bool sx = P.face[ex_(j) > 0 ? 0 : 1].ubc == U_SPECULAR;
+    const bool sy = P.face[ey_(j) > 0 ? 2 : 3].ubc == U_SPECULAR;
+    const bool sz = P.face[ez_(j) > 0 ? 4 : 5].ubc == U_SPECULAR;
+    const int ix = sx ? spec_(0, j) : opp_(j), iy = sy ? spec_(1, j) : opp_(j), iz = sz ? spec_(2, j) : opp_(j);
+    const int tx = sx ? opp_(spec_(0, j)) : j, ty = sy ? opp_(spec_(1, j)) : j, tz = sz ? opp_(spec_(2, j)) : j;
+    int bi = cx ? ix : -1;
+    slot = cx ? tx : 0;
+    if (cy && iy >= bi) { bi = iy; slot = ty; }
+    if (cz && iz >= bi) { bi = iz; slot = tz; }
+    return bi;
+}
+
+// Adds the moving-wall term of slot j of a wall cell to v, as gather() does
+// (same expression, so the FP32 contraction is the same).
+template <class R>
+__device__ __forceinline__ void add_moving_term(const SimParams& P, const Phys<R>& K, int j, bool cx, bool cy,
+                                                bool cz, R rho, R& v) {
+    int bf;
+    wall_source(P, j, cx, cy, cz, &bf);
+    if (P.face[bf].ubc == U_MOVING) {
+        const R dot = R(ex_(j)) * K.uw[bf][0] + R(ey_(j)) * K.uw[bf][1] + R(ez_(j)) * K.uw[bf][2];
+        v = v + R(6.0) * rho * w_<R>(j) * dot;
+    }
+}
+
+// Cell offsets of c + e (e = +1 / -1) along each axis, periodic wrap folded
+// in, and whether the cell is on the low / high face of each axis.
+template <class I>
+struct AxisOff {
+    I xm, xp, ym, yp, zm, zp;
+    bool lox, hix, loy, hiy, loz, hiz;
+};
+template <class I>
+__device__ __forceinline__ AxisOff<I> axis_off(const SimParams& P, CellPos q) {
+    AxisOff<I> o;
+    const int nx = P.nx, ny = P.ny, nz = P.nz;
+    const I nxy = (I)P.nxy;
+    o.lox = q.x == 0; o.hix = q.x == nx - 1; o.loy = q.y == 0; o.hiy = q.y == ny - 1;
+    o.loz = q.z == 0; o.hiz = q.z == nz - 1;
+    o.xm = o.lox ? (I)(nx - 1) : (I)-1;
+    o.xp = o.hix ? (I)(1 - nx) : (I)1;
+    o.ym = o.loy ? (I)(ny - 1) * nx : -(I)nx;
+    o.yp = o.hiy ? -(I)(ny - 1) * nx : (I)nx;
+    o.zm = o.loz ? (I)(nz - 1) * nxy : -nxy;
+    o.zp = o.hiz ? -(I)(nz - 1) * nxy : nxy;
+    return o;
+}
+// offset of c - e_j (source of a gather)
+template <class I>
+__device__ __forceinline__ I src_off(const AxisOff<I>& o, int j) {
+    return (ex_(j) > 0 ? o.xm : ex_(j) < 0 ? o.xp : (I)0) + (ey_(j) > 0 ? o.ym : ey_(j) < 0 ? o.yp : (I)0) +
+           (ez_(j) > 0 ? o.zm : ez_(j) < 0 ? o.zp : (I)0);
+}
+// does c - e_j lie beyond a wall, per axis
+template <class I>
+__device__ __forceinline__ void crossing(const SimParams& P, const AxisOff<I>& o, int j, bool& cx, bool& cy,
+                                         bool& cz) {
+    cx = !P.uper[0] && ((ex_(j) > 0 && o.lox) || (ex_(j) < 0 && o.hix));
+    cy = !P.uper[2] && ((ey_(j) > 0 && o.loy) || (ey_(j) < 0 && o.hiy));
+    cz = !P.uper[4] && ((ez_(j) > 0 && o.loz) || (ez_(j) < 0 && o.hiz));
+}
+
+template <class R, class S, bool DEV, bool WALLS, class I>
+__global__ void __launch_bounds__(256, lbm_min_blocks<R, S, WALLS>())
+    lbm_aa_even_kernel(const __grid_constant__ SimParams P, FastDiv dnx, FastDiv dnxy, S* F, const R* __restrict__ Fb,
+                       R* __restrict__ rho_buf, R* __restrict__ uout, int write_rho_all) {
+    const I c = (I)blockIdx.x * (I)blockDim.x + (I)threadIdx.x;
+    if (c >= (I)P.V) return;
+    const I V = (I)P.V;
+    const Phys<R>& K = phys_ref<R>(P);
+    S raw[15];
+#pragma unroll
+    for (int j = 0; j < 15; ++j) raw[j] = F[j * V + c];
+    R f[15];
+#pragma unroll
+    for (int j = 0; j < 15; ++j) f[j] = Store<S>::widen(raw[j]);
+    R rho, ux, uy, uz;
+    collide<R, DEV>(K, f, Fb[c], Fb[V + c], Fb[2 * V + c], rho, ux, uy, uz);
+#pragma unroll
+    for (int j = 0; j < 15; ++j) Store<S>::st(F + opp_(j) * V + c, f[j]);
+    uout[c] = ux;
+    uout[V + c] = uy;
+    uout[2 * V + c] = uz;
+    bool mv = false;
+    if (WALLS && P.moving_any && !write_rho_all) {
+        CellPos q;
+        q.z = (int)fdiv((uint32_t)c, dnxy);
+        const uint32_t r = (uint32_t)((int64_t)c - (int64_t)q.z * P.nxy);
+        q.y = (int)fdiv(r, dnx);
+        q.x = (int)(r - (uint32_t)q.y * (uint32_t)P.nx);
+        mv = touches_moving(P, q.x, q.y, q.z);
+    }
+    if (write_rho_all || mv) rho_buf[c] = rho;
+}
+
+template <class R, class S, bool DEV, bool WALLS, class I>
+__global__ void __launch_bounds__(256, lbm_min_blocks<R, S, WALLS>())
+    lbm_aa_odd_kernel(const __grid_constant__ SimParams P, FastDiv dnx, FastDiv dnxy, S* F, const R* __restrict__ Fb,
+                      R* __restrict__ rho_buf, R* __restrict__ uout, int write_rho_all) {
+    const I c = (I)blockIdx.x * (I)blockDim.x + (I)threadIdx.x;
+    if (c >= (I)P.V) return;
+    const I V = (I)P.V;
+    const Phys<R>& K = phys_ref<R>(P);
+    CellPos q;
+    q.z = (int)fdiv((uint32_t)c, dnxy);
+    const uint32_t r = (uint32_t)((int64_t)c - (int64_t)q.z * P.nxy);
+    q.y = (int)fdiv(r, dnx);
+    q.x = (int)(r - (uint32_t)q.y * (uint32_t)P.nx);
+    const AxisOff<I> o = axis_off<I>(P, q);
+    const bool mv = WALLS && P.moving_any && touches_moving(P, q.x, q.y, q.z);
+    const R rho_prev = mv ? rho_buf[c] : R(0);
+    // gather: all 15 loads issued before the first widening
+    S raw[15];
+#pragma unroll
+    for (int j = 0; j < 15; ++j) {
+        if constexpr (!WALLS) {
+            raw[j] = F[opp_(j) * V + c + src_off<I>(o, j)];
+        } else {
+            bool cx, cy, cz;
+            crossing<I>(P, o, j, cx, cy, cz);
+            int slot;
+            wall_bi(P, j, cx, cy, cz, slot);
+            const I src = (cx || cy || cz) ? (I)slot * V + c : (I)opp_(j) * V + c + src_off<I>(o, j);
+            raw[j] = F[src];
+        }
+    }
+    R f[15];
+#pragma unroll
+    for (int j = 0; j < 15; ++j) f[j] = Store<S>::widen(raw[j]);
+    if constexpr (WALLS) {
+        if (mv) {
+#pragma unroll
+            for (int j = 0; j < 15; ++j) {
+                bool cx, cy, cz;
+                crossing<I>(P, o, j, cx, cy, cz);
+                if (!(cx || cy || cz)) continue;
+                add_moving_term<R>(P, K, j, cx, cy, cz, rho_prev, f[j]);
+            }
+        }
+    }
+    R rho, ux, uy, uz;
+    collide<R, DEV>(K, f, Fb[c], Fb[V + c], Fb[2 * V + c], rho, ux, uy, uz);
+    // scatter
+#pragma unroll
+    for (int k = 0; k < 15; ++k) {
+        if constexpr (!WALLS) {
+            Store<S>::st(F + k * V + c + src_off<I>(o, opp_(k)), f[k]);  // c - e_opp(k) = c + e_k
+        } else {
+            // c + e_k beyond a wall <=> c - e_j beyond it for j = opp(k).  The
+            // wall value is chosen among the compile-time candidates of
+            // wall_bi (the largest source index wins), and the store address
+            // and value by selects, so wall lanes do not split the warp.
+            const int j = opp_(k);
+            bool cx, cy, cz;
+            crossing<I>(P, o, j, cx, cy, cz);
+            const bool sx = P.face[ex_(j) > 0 ? 0 : 1].ubc == U_SPECULAR;
+            const bool sy = P.face[ey_(j) > 0 ? 2 : 3].ubc == U_SPECULAR;
+            const bool sz = P.face[ez_(j) > 0 ? 4 : 5].ubc == U_SPECULAR;
+            const int ix = sx ? spec_(0, j) : opp_(j), iy = sy ? spec_(1, j) : opp_(j), iz = sz ? spec_(2, j) : opp_(j);
+            const R fx = sx ? f[spec_(0, j)] : f[opp_(j)], fy = sy ? f[spec_(1, j)] : f[opp_(j)];
+            const R fz = sz ? f[spec_(2, j)] : f[opp_(j)];
+            int bi = cx ? ix : -1;
+            R v = cx ? fx : f[k];
+            if (cy && iy >= bi) { bi = iy; v = fy; }
+            if (cz && iz >= bi) { v = fz; }
+            const bool cross = cx || cy || cz;
+            if (mv && cross) add_moving_term<R>(P, K, j, cx, cy, cz, rho, v);
+            Store<S>::st(F + (cross ? (I)j * V + c : (I)k * V + c + src_off<I>(o, j)), v);
+        }
+    }
+    uout[c] = ux;
+    uout[V + c] = uy;
+    uout[2 * V + c] = uz;
+    if (write_rho_all || mv) rho_buf[c] = rho;
+}
+
+// Pre-collision populations of direction j from a SWAP-layout buffer (for a
+// download of f): the odd step's gather of one direction.
+template <class R, class S>
+__device__ __forceinline__ R aa_pre_population(const SimParams& P, const Phys<R>& K, const S* F, int64_t c,
+                                               CellPos q, int j, const R* rho_buf) {
+    const int64_t V = P.V;
+    const AxisOff<int64_t> o = axis_off<int64_t>(P, q);
+    bool cx, cy, cz;
+    crossing<int64_t>(P, o, j, cx, cy, cz);
+    if (!(cx || cy || cz)) return Store<S>::widen(F[opp_(j) * V + c + src_off<int64_t>(o, j)]);
+    int slot;
+    wall_bi(P, j, cx, cy, cz, slot);
+    R v = Store<S>::widen(F[(int64_t)slot * V + c]);
+    if (P.moving_any && touches_moving(P, q.x, q.y, q.z)) add_moving_term<R>(P, K, j, cx, cy, cz, rho_buf[c], v);
+    return v;
+}
+
+// Download of direction dir from a SWAP-layout buffer, as float64 (the
+// deviation offset w_dir rho0 added back).
+template <class R, class S, bool DEV>
+__global__ void __launch_bounds__(256) aa_pop_out_kernel(const __grid_constant__ SimParams P, FastDiv dnx,
+                                                         FastDiv dnxy, const S* F, const R* __restrict__ rho_buf,
+                                                         double* __restrict__ dst, int dir) {
+    const int64_t c = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (c >= P.V) return;
+    CellPos q;
+    q.z = (int)fdiv((uint32_t)c, dnxy);
+    const uint32_t r = (uint32_t)(c - (int64_t)q.z * P.nxy);
+    q.y = (int)fdiv(r, dnx);
+    q.x = (int)(r - (uint32_t)q.y * (uint32_t)P.nx);
+    const R v = aa_pre_population<R, S>(P, phys_ref<R>(P), F, c, q, dir, rho_buf);
+    dst[c] = (double)v + (DEV ? w_<double>(dir) * P.kDensity : 0.0);
+}
+
+// In-place exchange of the direction slots j and opp(j) of every cell:
+// converts the post-collision populations between the two-buffer layout
+// (F[i][c] = f*_i(c)) and the SWAP layout (F[opp(i)][c] = f*_i(c)).
+template <class S>
+__global__ void __launch_bounds__(256) swap_pairs_kernel(int64_t V, S* F) {
+    const int64_t c = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (c >= V) return;
+#pragma unroll
+    for (int j = 1; j < 15; ++j) {
+        if (opp_(j) < j) continue;
+        const S a = F[j * V + c], b = F[opp_(j) * V + c];
+        F[j * V + c] = b;
+        F[opp_(j) * V + c] = a;
+    }
+}
+
 // Pre-collision populations from the stored post-collision ones (for a
 // download of f): the gather alone.
 template <class R, class S>
