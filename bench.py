@@ -380,6 +380,32 @@ def reference_cpu(workload, max_steps, warmup):
             "ms_step": dt * 1e3 / max_steps}
 
 
+REF_GPU_BUILD = {"periodic512": "b_p512", "slit64": "b_slit"}
+
+
+def reference_gpu(workload, steps=10, warmup=3):
+    """The reference's own FP64 CUDA solver (DeviceSolver<SimBC>, src/cuda,
+    built from its sources by oracle/build_ref.py) on the same seeded
+    workload, timed with CUDA events: the GPU baseline of the FP64 path."""
+    from oracle import build_ref
+    tag = REF_GPU_BUILD.get(workload)
+    exe = build_ref.gpu_bench_path(tag) if tag else None
+    if not exe or not os.path.exists(exe):
+        return {"value": None, "error": "reference GPU build absent for this workload"}
+    r = subprocess.run([exe, str(SEED), repr(S0), repr(SIGMA), str(warmup), str(steps)], capture_output=True,
+                       text=True, timeout=900)
+    d = json.loads(r.stdout.strip().splitlines()[-1])
+    if "error" in d:
+        return {"value": None, "error": d["error"][:300]}
+    nx, ny, nz, *_ = WORKLOADS[workload]
+    peak, _ = measured_peaks()
+    return {"value": d["mlups"], "unit": "MLUPS", "dtype": "f64", "steps": steps, "ms_per_step": d["ms_step"],
+            "ms_q_stage": d["ms_q"], "ms_lbm": d["ms_lbm"],
+            "note": "reference src/cuda kernels (GpuQTensorStep + GpuComputeBodyForce + GpuCollideAndStream), "
+                    "sm_100a build of its sources, default stream, CUDA events",
+            "frac_at_368B": 368 * nx * ny * nz / (d["ms_step"] * 1e-3) / 1e9 / peak}
+
+
 def ref_sample_steps(V, steps):
     """Steps of a bounded CPU sample: about half a minute of reference work."""
     return max(1, min(steps, 3 if V > 5e7 else 20 if V > 1e6 else 200))
@@ -513,6 +539,12 @@ def main():
             s2.close()
             torch.cuda.empty_cache()
         line["variants"] = variants
+        try:
+            line["reference_gpu"] = reference_gpu(a.workload)
+            if line["reference_gpu"].get("value") and "fp64" in variants:
+                line["reference_gpu"]["fp64_speedup"] = variants["fp64"]["value"] / line["reference_gpu"]["value"]
+        except Exception as e:  # reported, never required
+            line["reference_gpu"] = {"value": None, "error": str(e)[:300]}
         line["other_workloads"] = side_workloads([w for w in ("slit64", "channel20") if w != a.workload], local,
                                                  stream)
         line["ensemble"] = ensemble_vs_sequential(local, stream)

@@ -867,6 +867,20 @@ int lbman_set_shape(lbman_solver* s, const lbman_shape* sh) {
     return LBMAN_OK;
 }
 
+// Average step time of the current shape over n steps after one untimed
+// step, CUDA events on the solver's stream.
+static int time_trial(lbman_solver* s, int n, cudaEvent_t e0, cudaEvent_t e1, double* ms_per_step) {
+    LB_TRY(one_step(s, false));
+    cudaEventRecord(e0, s->stream);
+    for (int i = 0; i < n; ++i) LB_TRY(one_step(s, false));
+    cudaEventRecord(e1, s->stream);
+    if (cudaEventSynchronize(e1) != cudaSuccess) return fail(LBMAN_ERR_CUDA, "autotune trial failed");
+    float ms = 0.f;
+    cudaEventElapsedTime(&ms, e0, e1);
+    *ms_per_step = ms / n;
+    return LBMAN_OK;
+}
+
 int lbman_autotune(lbman_solver* s, int steps_per_trial, lbman_shape* best, int* ntrials) {
     if (!s || !best) return fail(LBMAN_ERR_ARG, "null argument");
     if (!s->uploaded) return fail(LBMAN_ERR_STATE, "autotune needs an uploaded state");
@@ -894,6 +908,7 @@ int lbman_autotune(lbman_solver* s, int steps_per_trial, lbman_shape* best, int*
     cudaEvent_t e0 = nullptr, e1 = nullptr;
     int status = LBMAN_OK, count = 0;
     lbman_shape orig, cur{}, win{};
+    std::vector<lbman_shape> trials;
     lbman_get_shape(s, &orig);
     win = orig;
     win.ms_per_step = 1e30;
@@ -922,22 +937,23 @@ int lbman_autotune(lbman_solver* s, int steps_per_trial, lbman_shape* best, int*
                     if (seen || (zi >= 6 && zs[zi] >= s->P.nz)) continue;
                     cur = {k, t[0], t[1], zs[zi], 0, 0.0};
                     if (lbman_set_shape(s, &cur) != LBMAN_OK) continue;
-                    if ((status = one_step(s, false)) != LBMAN_OK) break;
-                    cudaEventRecord(e0, s->stream);
-                    for (int n = 0; n < steps_per_trial && status == LBMAN_OK; ++n) status = one_step(s, false);
-                    cudaEventRecord(e1, s->stream);
-                    if (status != LBMAN_OK) break;
-                    if (cudaEventSynchronize(e1) != cudaSuccess) {
-                        status = fail(LBMAN_ERR_CUDA, "autotune trial failed");
-                        break;
-                    }
-                    float ms = 0.f;
-                    cudaEventElapsedTime(&ms, e0, e1);
-                    cur.ms_per_step = ms / steps_per_trial;
+                    if ((status = time_trial(s, steps_per_trial, e0, e1, &cur.ms_per_step)) != LBMAN_OK) break;
                     ++count;
-                    if (cur.ms_per_step < win.ms_per_step) win = cur;
+                    trials.push_back(cur);
                 }
             }
+        }
+        // Short trials are noisy (clocks move under the power cap): the best
+        // few are timed again with three times the steps and the winner is
+        // taken among them.
+        std::sort(trials.begin(), trials.end(),
+                  [](const lbman_shape& a, const lbman_shape& b) { return a.ms_per_step < b.ms_per_step; });
+        for (size_t i = 0; i < trials.size() && i < 4 && status == LBMAN_OK; ++i) {
+            cur = trials[i];
+            if (lbman_set_shape(s, &cur) != LBMAN_OK) continue;
+            if ((status = time_trial(s, 3 * steps_per_trial, e0, e1, &cur.ms_per_step)) != LBMAN_OK) break;
+            ++count;
+            if (cur.ms_per_step < win.ms_per_step) win = cur;
         }
     }
     // Restore the state and the indices it lived in, then adopt the winner.

@@ -251,20 +251,25 @@ cudaError_t lbm_aa(const SimParams& P, bool odd, bool wr, void* f, const void* F
     auto launch = [&](auto kern) {
         kern<<<nb, 256, 0, st>>>(P, dnx, dnxy, (S*)f, (const R*)F, (R*)rho, (R*)uout, wr ? 1 : 0);
     };
-    const bool walls = !(P.uper[0] && P.uper[2] && P.uper[4]);
+    // walled axes (a velocity axis is periodic on both faces or on neither):
+    // none, x only (slit), x and y (channel), or any
+    const int wm = (P.uper[0] ? 0 : 1) | (P.uper[2] ? 0 : 2) | (P.uper[4] ? 0 : 4);
     const bool i32 = 15 * P.V < ((int64_t)1 << 31);
 #define LBMAN_AA(W, I)                                                        \
     do {                                                                      \
         if (odd) launch(lbm_aa_odd_kernel<R, S, DEV, W, I>);                  \
         else launch(lbm_aa_even_kernel<R, S, DEV, W, I>);                     \
     } while (0)
-    if (walls) {
-        if (i32) LBMAN_AA(true, int);
-        else LBMAN_AA(true, int64_t);
-    } else {
-        if (i32) LBMAN_AA(false, int);
-        else LBMAN_AA(false, int64_t);
-    }
+#define LBMAN_AA_I(W)                                                         \
+    do {                                                                      \
+        if (i32) LBMAN_AA(W, int);                                            \
+        else LBMAN_AA(W, int64_t);                                            \
+    } while (0)
+    if (wm == 0) LBMAN_AA_I(0);
+    else if (wm == 1) LBMAN_AA_I(1);
+    else if ((wm & ~3) == 0) LBMAN_AA_I(3);
+    else LBMAN_AA_I(7);
+#undef LBMAN_AA_I
 #undef LBMAN_AA
     return cudaGetLastError();
 }

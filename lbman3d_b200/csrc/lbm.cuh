@@ -390,17 +390,19 @@ __device__ __forceinline__ I src_off(const AxisOff<I>& o, int j) {
     return (ex_(j) > 0 ? o.xm : ex_(j) < 0 ? o.xp : (I)0) + (ey_(j) > 0 ? o.ym : ey_(j) < 0 ? o.yp : (I)0) +
            (ez_(j) > 0 ? o.zm : ez_(j) < 0 ? o.zp : (I)0);
 }
-// does c - e_j lie beyond a wall, per axis
-template <class I>
+// does c - e_j lie beyond a wall, per axis.  WM: the axes that may have
+// walls (bit 0 x, 1 y, 2 z), a compile-time superset of the box's walled
+// axes, so directions and axes that cannot cross cost nothing.
+template <int WM, class I>
 __device__ __forceinline__ void crossing(const SimParams& P, const AxisOff<I>& o, int j, bool& cx, bool& cy,
                                          bool& cz) {
-    cx = !P.uper[0] && ((ex_(j) > 0 && o.lox) || (ex_(j) < 0 && o.hix));
-    cy = !P.uper[2] && ((ey_(j) > 0 && o.loy) || (ey_(j) < 0 && o.hiy));
-    cz = !P.uper[4] && ((ez_(j) > 0 && o.loz) || (ez_(j) < 0 && o.hiz));
+    cx = (WM & 1) && ex_(j) != 0 && !P.uper[0] && ((ex_(j) > 0 && o.lox) || (ex_(j) < 0 && o.hix));
+    cy = (WM & 2) && ey_(j) != 0 && !P.uper[2] && ((ey_(j) > 0 && o.loy) || (ey_(j) < 0 && o.hiy));
+    cz = (WM & 4) && ez_(j) != 0 && !P.uper[4] && ((ez_(j) > 0 && o.loz) || (ez_(j) < 0 && o.hiz));
 }
 
-template <class R, class S, bool DEV, bool WALLS, class I>
-__global__ void __launch_bounds__(256, lbm_min_blocks<R, S, WALLS>())
+template <class R, class S, bool DEV, int WM, class I>
+__global__ void __launch_bounds__(256, lbm_min_blocks<R, S, WM != 0>())
     lbm_aa_even_kernel(const __grid_constant__ SimParams P, FastDiv dnx, FastDiv dnxy, S* F, const R* __restrict__ Fb,
                        R* __restrict__ rho_buf, R* __restrict__ uout, int write_rho_all) {
     const I c = (I)blockIdx.x * (I)blockDim.x + (I)threadIdx.x;
@@ -421,7 +423,7 @@ __global__ void __launch_bounds__(256, lbm_min_blocks<R, S, WALLS>())
     uout[V + c] = uy;
     uout[2 * V + c] = uz;
     bool mv = false;
-    if (WALLS && P.moving_any && !write_rho_all) {
+    if (WM != 0 && P.moving_any && !write_rho_all) {
         CellPos q;
         q.z = (int)fdiv((uint32_t)c, dnxy);
         const uint32_t r = (uint32_t)((int64_t)c - (int64_t)q.z * P.nxy);
@@ -432,8 +434,8 @@ __global__ void __launch_bounds__(256, lbm_min_blocks<R, S, WALLS>())
     if (write_rho_all || mv) rho_buf[c] = rho;
 }
 
-template <class R, class S, bool DEV, bool WALLS, class I>
-__global__ void __launch_bounds__(256, lbm_min_blocks<R, S, WALLS>())
+template <class R, class S, bool DEV, int WM, class I>
+__global__ void __launch_bounds__(256, lbm_min_blocks<R, S, WM != 0>())
     lbm_aa_odd_kernel(const __grid_constant__ SimParams P, FastDiv dnx, FastDiv dnxy, S* F, const R* __restrict__ Fb,
                       R* __restrict__ rho_buf, R* __restrict__ uout, int write_rho_all) {
     const I c = (I)blockIdx.x * (I)blockDim.x + (I)threadIdx.x;
@@ -446,6 +448,7 @@ __global__ void __launch_bounds__(256, lbm_min_blocks<R, S, WALLS>())
     q.y = (int)fdiv(r, dnx);
     q.x = (int)(r - (uint32_t)q.y * (uint32_t)P.nx);
     const AxisOff<I> o = axis_off<I>(P, q);
+    constexpr bool WALLS = WM != 0;
     const bool mv = WALLS && P.moving_any && touches_moving(P, q.x, q.y, q.z);
     const R rho_prev = mv ? rho_buf[c] : R(0);
     // gather: all 15 loads issued before the first widening
@@ -456,7 +459,7 @@ __global__ void __launch_bounds__(256, lbm_min_blocks<R, S, WALLS>())
             raw[j] = F[opp_(j) * V + c + src_off<I>(o, j)];
         } else {
             bool cx, cy, cz;
-            crossing<I>(P, o, j, cx, cy, cz);
+            crossing<WM, I>(P, o, j, cx, cy, cz);
             int slot;
             wall_bi(P, j, cx, cy, cz, slot);
             const I src = (cx || cy || cz) ? (I)slot * V + c : (I)opp_(j) * V + c + src_off<I>(o, j);
@@ -471,7 +474,7 @@ __global__ void __launch_bounds__(256, lbm_min_blocks<R, S, WALLS>())
 #pragma unroll
             for (int j = 0; j < 15; ++j) {
                 bool cx, cy, cz;
-                crossing<I>(P, o, j, cx, cy, cz);
+                crossing<WM, I>(P, o, j, cx, cy, cz);
                 if (!(cx || cy || cz)) continue;
                 add_moving_term<R>(P, K, j, cx, cy, cz, rho_prev, f[j]);
             }
@@ -491,7 +494,7 @@ __global__ void __launch_bounds__(256, lbm_min_blocks<R, S, WALLS>())
             // and value by selects, so wall lanes do not split the warp.
             const int j = opp_(k);
             bool cx, cy, cz;
-            crossing<I>(P, o, j, cx, cy, cz);
+            crossing<WM, I>(P, o, j, cx, cy, cz);
             const bool sx = P.face[ex_(j) > 0 ? 0 : 1].ubc == U_SPECULAR;
             const bool sy = P.face[ey_(j) > 0 ? 2 : 3].ubc == U_SPECULAR;
             const bool sz = P.face[ez_(j) > 0 ? 4 : 5].ubc == U_SPECULAR;
@@ -521,7 +524,7 @@ __device__ __forceinline__ R aa_pre_population(const SimParams& P, const Phys<R>
     const int64_t V = P.V;
     const AxisOff<int64_t> o = axis_off<int64_t>(P, q);
     bool cx, cy, cz;
-    crossing<int64_t>(P, o, j, cx, cy, cz);
+    crossing<7, int64_t>(P, o, j, cx, cy, cz);
     if (!(cx || cy || cz)) return Store<S>::widen(F[opp_(j) * V + c + src_off<int64_t>(o, j)]);
     int slot;
     wall_bi(P, j, cx, cy, cz, slot);

@@ -109,11 +109,20 @@ def params_h(cfg: dict) -> str:
 
 def sim_config_h(cfg: dict) -> str:
     adv = cfg.get("advection", "Centred")
+    bc = cfg.get("bc", "FullyPeriodicConfig")
+    extra = []
+    if bc == "SlitFreeSlipConfig":  # the reference's SlitConfig (src/sim_config.h:19-27)
+        extra = ["struct SlitFreeSlipConfig {",
+                 "    using XLo = WallSpec<Neumann, SpecularReflection>;",
+                 "    using XHi = WallSpec<Neumann, SpecularReflection>;",
+                 "    using YLo = WallSpec<Periodic, Periodic>;", "    using YHi = WallSpec<Periodic, Periodic>;",
+                 "    using ZLo = WallSpec<Periodic, Periodic>;", "    using ZHi = WallSpec<Periodic, Periodic>;",
+                 "};"]
     return "\n".join([
         "// Generated by oracle/build_ref.py -- shadows src/sim_config.h.",
         "#ifndef LBM_AN_SIM_CONFIG_H_", "#define LBM_AN_SIM_CONFIG_H_",
-        "#include \"boundary.h\"", "#include \"qtensor_types.h\"",
-        "using SimBC = FullyPeriodicConfig;",
+        "#include \"boundary.h\"", "#include \"qtensor_types.h\""] + extra + [
+        f"using SimBC = {bc};",
         f"inline constexpr Advection kQAdvection = Advection::{adv};",
         "inline constexpr int kNumSteps = 1;", "inline constexpr int kSaveInterval = 1;",
         "#endif", ""])
@@ -144,6 +153,46 @@ def build(tag: str, cfg: dict, verbose: bool = False) -> str:
     # The reference's release flags (CMakeLists.txt:59-60).
     cmd = ["g++", "-std=c++23", "-O3", "-DNDEBUG", "-fopenmp", "-w",
            "-I", d, "-I", REF_SRC, "-I", HERE, "-o", exe] + srcs + [gen, "-lm"]
+    if verbose:
+        print(" ".join(cmd))
+    subprocess.run(cmd, check=True)
+    return exe
+
+
+# Parameter sets of the reference's own CUDA solver timing (ref_gpu_bench.cu):
+# the reference's src/cuda sources compiled for sm_100a.
+GPU_BUILDS = {
+    "b_p512": dict(nx=512, ny=512, nz=512, ALPHA=0.01),
+    "b_slit": dict(nx=64, ny=256, nz=256, ALPHA=0.01, bc="SlitFreeSlipConfig"),
+}
+
+
+def gpu_bench_path(tag: str) -> str:
+    return os.path.join(OUT, tag + "_gpu", "ref_gpu_bench")
+
+
+def build_gpu(tag: str, cfg: dict, verbose: bool = False) -> str:
+    """ref_gpu_bench for one parameter set: the reference's DeviceFields /
+    DeviceSolver / kernels (src/cuda), nvcc for sm_100a with -DNDEBUG (the
+    reference's release flags; its device-side index asserts compiled out)."""
+    if not os.path.isdir(REF_SRC):
+        raise FileNotFoundError(f"{REF_SRC} is not present; oracle/_ref cannot be rebuilt here")
+    d = os.path.join(OUT, tag + "_gpu")
+    os.makedirs(d, exist_ok=True)
+    with open(os.path.join(d, "params.h"), "w") as fh:
+        fh.write(params_h(cfg))
+    with open(os.path.join(d, "sim_config.h"), "w") as fh:
+        fh.write(sim_config_h(cfg))
+    gen = os.path.join(d, "lbman_oracle.o")
+    subprocess.run(["gcc", "-std=c11", "-O2", "-ffp-contract=off", "-fopenmp", "-c", os.path.join(HERE, "lbman_oracle.c"),
+                    "-o", gen], check=True)
+    exe = gpu_bench_path(tag)
+    srcs = [os.path.join(HERE, "ref_gpu_bench.cu"), os.path.join(REF_SRC, "cuda", "device_fields.cu"),
+            os.path.join(REF_SRC, "cuda", "device_solver.cu"), os.path.join(REF_SRC, "fluid_fields.cc"),
+            os.path.join(REF_SRC, "qtensor_fields.cc")]
+    cmd = [os.environ.get("NVCC", "nvcc"), "-gencode", "arch=compute_100a,code=sm_100a", "-std=c++20", "-O3",
+           "-DNDEBUG", "-DSIM_WITH_CUDA", "-w", "-Xcompiler", "-fopenmp", "-I", d, "-I", REF_SRC,
+           "-I", os.path.join(REF_SRC, "cuda"), "-I", HERE, "-o", exe] + srcs + [gen, "-lgomp"]
     if verbose:
         print(" ".join(cmd))
     subprocess.run(cmd, check=True)
@@ -192,9 +241,12 @@ def main(argv=None) -> int:
         for k, v in REF_BUILDS.items():
             print(k, v)
         return 0
-    tags = a.tags or list(REF_BUILDS) + list(DROPIN_BUILDS)
+    tags = a.tags or list(REF_BUILDS) + list(DROPIN_BUILDS) + [t + "_gpu" for t in GPU_BUILDS]
     for t in tags:
-        if t in DROPIN_BUILDS:
+        if t.endswith("_gpu") and t[:-4] in GPU_BUILDS:
+            build_gpu(t[:-4], GPU_BUILDS[t[:-4]], a.v)
+            print("built", gpu_bench_path(t[:-4]))
+        elif t in DROPIN_BUILDS:
             build_dropin(t, DROPIN_BUILDS[t], a.v)
             print("built", dropin_path(t))
         else:
