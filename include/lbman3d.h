@@ -235,6 +235,75 @@ int lbman_set_shape(lbman_solver* s, const lbman_shape* shape);
  * timed.                                                                    */
 int lbman_autotune(lbman_solver* s, int steps_per_trial, lbman_shape* best, int* ntrials);
 
+/* z-slab decomposition of one box across GPUs (or across handles on one GPU).
+ * Replaces the reference's MPI domain decomposition (src/mpi/mpi_context.h,
+ * src/mpi/halo_exchange_qtensor.h:131-209, src/mpi/halo_exchange_lbm.h:
+ * 304-386) for the single split axis z.
+ *
+ * lbman_create_slab makes a handle that owns planes [z_offset, z_offset +
+ * cfg->nz) of a box of nz_global planes (cfg->nz >= 2).  The box's z faces
+ * must be periodic (every reference preset: FullyPeriodic, Channel, Slit,
+ * SlitNoSlip); x and y keep any wall.  The handle allocates two ghost planes
+ * on each side and steps with the in-place organisations (LBMAN_KERNELS_SPLIT
+ * or _SPLIT_PAIR; AUTO means SPLIT).  upload / download / init_seeded take
+ * the owned planes (V = nx*ny*cfg->nz); init_seeded gives the owned planes
+ * of the whole box's seeded field.  Slabs i-1 and i+1 (mod the slab count)
+ * are the neighbours across the low and high z face.
+ *
+ * A step is three exchanges around the two kernel calls:
+ *   exchange LBMAN_HALO_QU; lbman_qtensor_step;
+ *   exchange LBMAN_HALO_F_IN; lbman_lbm_step; exchange LBMAN_HALO_F_OUT.
+ * The Q+force kernel computes the passive stresses of the ghost planes
+ * itself from the 2-deep Q/u halo, so no stress halo is exchanged.  The
+ * population exchanges move the 5 crossing directions of one plane and only
+ * around odd in-place steps (even steps are local); lbman_halo_spans returns
+ * n = 0 when the phase has nothing to move.  F_OUT lands in a staging area
+ * and lbman_halo_done merges it, keeping the slots that this slab's own
+ * x / y wall rule wrote (the reference's unpack skip rule).  Calls out of
+ * this order return LBMAN_ERR_STATE; lbman_step and the two-phase Q stage
+ * are not available on slabs; lbman_reduce on a slab sums its owned planes
+ * (LBMAN_DIAG_ENERGY needs a fresh QU halo; defects are not counted).      */
+#define LBMAN_HALO_QU 0    /* Q (5), u (3): 2 owned planes -> neighbour ghosts  */
+#define LBMAN_HALO_F_IN 1  /* 5 populations: owned plane -> neighbour ghost     */
+#define LBMAN_HALO_F_OUT 2 /* 5 populations: ghost plane -> neighbour's owned   */
+#define LBMAN_HALO_MAX_SPANS 8
+
+#define LBMAN_FIELD_Q 0      /* component 0-4 of the current Q              */
+#define LBMAN_FIELD_U 1      /* component 0-2 of the current velocity       */
+#define LBMAN_FIELD_F 2      /* population slot 0-14 (stored form)          */
+#define LBMAN_FIELD_FSTAGE 3 /* F_OUT staging: slot 0-4 of face `plane`     */
+
+/* One contiguous span of an exchange: `planes` planes of one component,
+ * starting at `plane` in owned coordinates (owned 0 .. nz_local-1, ghosts
+ * -2, -1 and nz_local, nz_local+1).                                        */
+typedef struct {
+    int field;
+    int comp;
+    int plane;
+    int planes;
+} lbman_halo_span;
+
+int lbman_create_slab(const lbman_config* cfg, int nz_global, int z_offset, lbman_solver** out);
+/* The spans of an exchange phase for a slab of nz_local planes (host only).
+ * send[f][k] goes to the neighbour across face f (0 = low z, 1 = high z),
+ * which receives it into its recv[1-f][k]; n spans per face (8 for QU, 5 for
+ * the population phases).                                                   */
+int lbman_halo_plan(int nz_local, int phase, lbman_halo_span send[2][LBMAN_HALO_MAX_SPANS],
+                    lbman_halo_span recv[2][LBMAN_HALO_MAX_SPANS], int* n);
+/* The plan's spans as device addresses of this slab's current buffers, all
+ * span_bytes long; n = 0 when the phase moves nothing now.  A transport
+ * (NCCL send/recv, peer copies) delivers them, then calls lbman_halo_done. */
+int lbman_halo_spans(lbman_solver* s, int phase, void* send[2][LBMAN_HALO_MAX_SPANS],
+                     void* recv[2][LBMAN_HALO_MAX_SPANS], size_t* span_bytes, int* n);
+int lbman_halo_done(lbman_solver* s, int phase);
+/* In-process transport: slabs[0..n-1] in z order (same or different
+ * devices), each slab's spans copied into its neighbours' with
+ * cudaMemcpyAsync on the receivers' streams, ordered by events (no host
+ * synchronisation), then lbman_halo_done on every slab.                    */
+int lbman_slab_exchange(lbman_solver* const* slabs, int nslabs, int phase);
+/* nz_global, z_offset, nz_local of a slab (0, 0, nz for a whole box).       */
+int lbman_slab_info(lbman_solver* s, int* nz_global, int* z_offset, int* nz_local);
+
 /* Ensemble runner (no counterpart in the reference, whose solver advances one
  * box per process).  Many independent boxes -- each with its own lbman_config
  * (size, boundary faces, physical parameters) -- advance together: every time

@@ -13,6 +13,7 @@ from .device import (DeviceFields, DeviceSolver, InitializeComputeBackend, LbmSo
 from .fields import FluidFields, LocalGrid, QTensorFields
 from .ensemble import Ensemble, draw_boxes
 from .params import Advection, EquilibriumScalarOrder, Params, Precision
+from .slab import DistributedSlab, Slab, SlabBox, split_planes
 
 __all__ = [
     "Anchoring", "BCConfig", "ChannelConfig", "FullyPeriodicConfig", "MovingWall", "Neumann", "NoSlip",
@@ -20,5 +21,5 @@ __all__ = [
     "from_face_tuples", "is_wall_by_face", "periodicity_by_axis", "DeviceFields", "DeviceSolver",
     "InitializeComputeBackend", "LbmSolver", "QTensorSolver", "Simulation", "make_config", "FluidFields",
     "LocalGrid", "QTensorFields", "Advection", "EquilibriumScalarOrder", "Params", "Precision", "Ensemble",
-    "draw_boxes",
+    "draw_boxes", "DistributedSlab", "Slab", "SlabBox", "split_planes",
 ]

@@ -18,6 +18,9 @@ CENTRED, UPWIND = 0, 1
 FP64, FP32, FP16 = 0, 1, 2
 KERNELS_AUTO, KERNELS_SPLIT, KERNELS_FUSED, KERNELS_SPLIT_PAIR = 0, 1, 2, 3
 DIAG_FLOW, DIAG_ENERGY, DIAG_DEFECTS, DIAG_ALL = 1, 2, 4, 7
+HALO_QU, HALO_F_IN, HALO_F_OUT = 0, 1, 2
+HALO_MAX_SPANS = 8
+FIELD_Q, FIELD_U, FIELD_F, FIELD_FSTAGE = 0, 1, 2, 3
 
 
 class lbman_face(C.Structure):
@@ -49,6 +52,10 @@ class lbman_shape(C.Structure):
 
 class lbman_defects(C.Structure):
     _fields_ = [("faces", C.c_int64), ("edges", C.c_int64), ("lines", C.c_int64), ("points", C.c_int64)]
+
+
+class lbman_halo_span(C.Structure):
+    _fields_ = [("field", C.c_int), ("comp", C.c_int), ("plane", C.c_int), ("planes", C.c_int)]
 
 
 class lbman_stats(C.Structure):
@@ -142,6 +149,14 @@ PROTOTYPES = [
     ("lbman_closure_step", C.c_int, [C.c_void_p, C.c_void_p, C.c_int]),
     ("lbman_closure_set_options", C.c_int, [C.c_void_p, C.c_float, C.c_float]),
     ("lbman_closure_set_wait_limit", C.c_int, [C.c_void_p, C.c_uint32]),
+    ("lbman_create_slab", C.c_int, [C.POINTER(lbman_config), C.c_int, C.c_int, C.POINTER(C.c_void_p)]),
+    ("lbman_halo_plan", C.c_int, [C.c_int, C.c_int, C.POINTER(lbman_halo_span), C.POINTER(lbman_halo_span),
+                                  C.POINTER(C.c_int)]),
+    ("lbman_halo_spans", C.c_int, [C.c_void_p, C.c_int, C.POINTER(C.c_void_p), C.POINTER(C.c_void_p),
+                                   C.POINTER(C.c_size_t), C.POINTER(C.c_int)]),
+    ("lbman_halo_done", C.c_int, [C.c_void_p, C.c_int]),
+    ("lbman_slab_exchange", C.c_int, [C.POINTER(C.c_void_p), C.c_int, C.c_int]),
+    ("lbman_slab_info", C.c_int, [C.c_void_p, C.POINTER(C.c_int), C.POINTER(C.c_int), C.POINTER(C.c_int)]),
     ("lbman_flow_reduce_noalloc", C.c_int,
      [C.c_int64, C.c_int, C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p, C.POINTER(lbman_diag)]),
 ]

@@ -54,6 +54,7 @@ struct Ops {
     decltype(&launch_lbm_aa_f64) lbm_aa;
     decltype(&launch_aa_pop_out_f64) aa_pop_out;
     decltype(&launch_swap_pairs_f64) swap_pairs;
+    decltype(&launch_halo_merge_f64) halo_merge;
     decltype(&launch_feq_init_f64) feq_init;
     decltype(&launch_pop_in_f64) pop_in;
     decltype(&launch_pop_out_f64) pop_out;
@@ -77,6 +78,7 @@ struct Ops {
     Ops {                                                                                              \
         launch_qforce_##SUF, launch_fused_##SUF, launch_lbm_##SUF, launch_stream_only_##SUF,           \
             launch_lbm_aa_##SUF, launch_aa_pop_out_##SUF, launch_swap_pairs_##SUF,                     \
+            launch_halo_merge_##SUF,                                                                   \
             launch_feq_init_##SUF, launch_pop_in_##SUF, launch_pop_out_##SUF, launch_real_in_##SUF,    \
             launch_real_out_##SUF, launch_flow_reduce_##SUF, launch_energy_reduce_##SUF,               \
             launch_director_##SUF, launch_defect_count_##SUF, launch_defect_flags_##SUF,              \
@@ -117,6 +119,11 @@ void build_sim_params(const lbman_config& c, SimParams& P) {
     P.nx = c.nx; P.ny = c.ny; P.nz = c.nz;
     P.nxy = (int64_t)c.nx * c.ny;
     P.V = P.nxy * c.nz;
+    P.zlo = 0;
+    P.zhi = c.nz;
+    P.c0 = 0;
+    P.c1 = P.V;
+    P.gbase = 0;
     P.DT = c.DT; P.kDensity = c.kDensity; P.L = c.L; P.A = c.A; P.B = c.B; P.C = c.C;
     P.LAMBDA = c.LAMBDA; P.GAMMA = c.GAMMA; P.ALPHA = c.ALPHA; P.MU = c.MU;
     // src/params.h:52-54
@@ -169,6 +176,17 @@ struct lbman_solver {
     // the fused organisation has run.
     int fphase = 0;
     bool uploaded = false;
+    // z-slab of a larger box (lbman_create_slab): owned planes [P.zlo, P.zhi)
+    // of an allocation with two ghost planes on each side.  The flags order
+    // the exchanges around the steps: the Q/u halo is fresh (exchanged since
+    // the last step), the population halo of an odd step is in, and the
+    // populations an odd step scattered into the ghost planes are still to
+    // be merged by the neighbours.
+    bool slab = false;
+    int nz_global = 0, z_offset = 0;
+    void* fstage = nullptr;  // F_OUT arrivals: 2 faces x 5 slots x nx*ny
+    bool qu_fresh = false, fin_fresh = false, fout_pending = false;
+    cudaEvent_t ev_ready = nullptr, ev_done = nullptr;
     cudaStream_t stream = nullptr;
     bool own_stream = false;
     int64_t steps = 0, launches = 0;
@@ -425,7 +443,9 @@ int lbman_destroy(lbman_solver* s) {
     if (s->stream) cudaStreamSynchronize(s->stream);
     for (int b = 0; b < 2; ++b) { cudaFree(s->f[b]); cudaFree(s->q[b]); cudaFree(s->u[b]); }
     cudaFree(s->rho); cudaFree(s->F); cudaFree(s->staging); cudaFree(s->partials); cudaFree(s->red_dev);
-    cudaFree(s->upast); cudaFree(s->dirbuf); cudaFree(s->stress);
+    cudaFree(s->upast); cudaFree(s->dirbuf); cudaFree(s->stress); cudaFree(s->fstage);
+    if (s->ev_ready) cudaEventDestroy(s->ev_ready);
+    if (s->ev_done) cudaEventDestroy(s->ev_done);
     lbman::stats::destroy(s->stats);
     if (s->red_host) cudaFreeHost(s->red_host);
     if (s->own_stream && s->stream) cudaStreamDestroy(s->stream);
@@ -454,21 +474,23 @@ int lbman_upload(lbman_solver* s, const double* rho, const double* u3, const dou
                  const double* force3) {
     if (!s || !rho || !u3 || !q5) return fail(LBMAN_ERR_ARG, "rho, u and q are required");
     LB_TRY(set_device(s));
-    const int64_t V = s->P.V;
-    LB_TRY(stage_in_real(s, rho, s->rho, V));
-    for (int k = 0; k < 3; ++k) LB_TRY(stage_in_real(s, u3 + k * V, vptr(s->u[s->ucur], k * V, s->rbytes), V));
-    for (int k = 0; k < 5; ++k) LB_TRY(stage_in_real(s, q5 + k * V, vptr(s->q[s->qcur], k * V, s->rbytes), V));
+    // host arrays hold the owned cells [c0, c1) (the whole box unless a slab)
+    const int64_t V = s->P.V, c0 = s->P.c0, Vo = s->P.c1 - s->P.c0;
+    LB_TRY(stage_in_real(s, rho, vptr(s->rho, c0, s->rbytes), Vo));
+    for (int k = 0; k < 3; ++k) LB_TRY(stage_in_real(s, u3 + k * Vo, vptr(s->u[s->ucur], k * V + c0, s->rbytes), Vo));
+    for (int k = 0; k < 5; ++k) LB_TRY(stage_in_real(s, q5 + k * Vo, vptr(s->q[s->qcur], k * V + c0, s->rbytes), Vo));
     if (force3) {
-        for (int k = 0; k < 3; ++k) LB_TRY(stage_in_real(s, force3 + k * V, vptr(s->F, k * V, s->rbytes), V));
+        for (int k = 0; k < 3; ++k) LB_TRY(stage_in_real(s, force3 + k * Vo, vptr(s->F, k * V + c0, s->rbytes), Vo));
     } else {
         LB_CUDA(cudaMemsetAsync(s->F, 0, 3 * V * s->rbytes, s->stream));
     }
     if (f15) {
         for (int j = 0; j < 15; ++j) {
             if (s->prec == LBMAN_FP64) {
-                LB_CUDA(cudaMemcpyAsync(vptr(s->f[s->fcur], j * V, 8), f15 + j * V, V * 8, cudaMemcpyHostToDevice, s->stream));
+                LB_CUDA(cudaMemcpyAsync(vptr(s->f[s->fcur], j * V + c0, 8), f15 + j * Vo, Vo * 8, cudaMemcpyHostToDevice,
+                                        s->stream));
             } else {
-                LB_CUDA(cudaMemcpyAsync(s->staging, f15 + j * V, V * 8, cudaMemcpyHostToDevice, s->stream));
+                LB_CUDA(cudaMemcpyAsync(s->staging + c0, f15 + j * Vo, Vo * 8, cudaMemcpyHostToDevice, s->stream));
                 LB_TRY(check_launch(s, s->ops().pop_in(s->P, s->staging, s->f[s->fcur], j, s->stream), "pop_in"));
             }
         }
@@ -479,6 +501,7 @@ int lbman_upload(lbman_solver* s, const double* rho, const double* u3, const dou
     s->uploaded = true;
     s->fphase = F_PRE;
     s->steps = 0;
+    s->qu_fresh = s->fin_fresh = s->fout_pending = false;
     return LBMAN_OK;
 }
 
@@ -537,18 +560,26 @@ int lbman_init_seeded(lbman_solver* s, uint64_t seed, double S0, double sigma) {
     s->uploaded = true;
     s->fphase = F_PRE;
     s->steps = 0;
+    s->qu_fresh = s->fin_fresh = s->fout_pending = false;
     return LBMAN_OK;
 }
 
 int lbman_download(lbman_solver* s, double* rho, double* u3, double* q5, double* f15, double* force3) {
     if (!s) return fail(LBMAN_ERR_ARG, "null solver");
     if (!s->uploaded) return fail(LBMAN_ERR_STATE, "download before upload");
+    if (s->slab && s->fout_pending)
+        return fail(LBMAN_ERR_STATE, "exchange LBMAN_HALO_F_OUT after an odd step before downloading a slab");
+    if (s->slab && f15 && s->fphase == F_SWAP && !s->fin_fresh)
+        return fail(LBMAN_ERR_STATE, "exchange LBMAN_HALO_F_IN before downloading a slab's populations here");
     LB_TRY(set_device(s));
-    const int64_t V = s->P.V;
-    if (rho) LB_TRY(stage_out_real(s, s->rho, rho, V));
-    if (u3) for (int k = 0; k < 3; ++k) LB_TRY(stage_out_real(s, vptr(s->u[s->ucur], k * V, s->rbytes), u3 + k * V, V));
-    if (q5) for (int k = 0; k < 5; ++k) LB_TRY(stage_out_real(s, vptr(s->q[s->qcur], k * V, s->rbytes), q5 + k * V, V));
-    if (force3) for (int k = 0; k < 3; ++k) LB_TRY(stage_out_real(s, vptr(s->F, k * V, s->rbytes), force3 + k * V, V));
+    const int64_t V = s->P.V, c0 = s->P.c0, Vo = s->P.c1 - s->P.c0;
+    if (rho) LB_TRY(stage_out_real(s, vptr(s->rho, c0, s->rbytes), rho, Vo));
+    if (u3)
+        for (int k = 0; k < 3; ++k) LB_TRY(stage_out_real(s, vptr(s->u[s->ucur], k * V + c0, s->rbytes), u3 + k * Vo, Vo));
+    if (q5)
+        for (int k = 0; k < 5; ++k) LB_TRY(stage_out_real(s, vptr(s->q[s->qcur], k * V + c0, s->rbytes), q5 + k * Vo, Vo));
+    if (force3)
+        for (int k = 0; k < 3; ++k) LB_TRY(stage_out_real(s, vptr(s->F, k * V + c0, s->rbytes), force3 + k * Vo, Vo));
     if (f15) {
         const void* src = s->f[s->fcur];
         if (s->fphase == F_POST) {  // stream the stored f* into the spare buffer
@@ -559,12 +590,13 @@ int lbman_download(lbman_solver* s, double* rho, double* u3, double* q5, double*
             if (s->fphase == F_SWAP) {  // the odd step's gather of direction j
                 if (!s->staging) return fail(LBMAN_ERR_STATE, "no staging buffer");
                 LB_TRY(check_launch(s, s->ops().aa_pop_out(s->P, src, s->rho, s->staging, j, s->stream), "aa_pop_out"));
-                LB_CUDA(cudaMemcpyAsync(f15 + j * V, s->staging, V * 8, cudaMemcpyDeviceToHost, s->stream));
+                LB_CUDA(cudaMemcpyAsync(f15 + j * Vo, s->staging + c0, Vo * 8, cudaMemcpyDeviceToHost, s->stream));
             } else if (s->prec == LBMAN_FP64) {
-                LB_CUDA(cudaMemcpyAsync(f15 + j * V, vptr((void*)src, j * V, 8), V * 8, cudaMemcpyDeviceToHost, s->stream));
+                LB_CUDA(cudaMemcpyAsync(f15 + j * Vo, vptr((void*)src, j * V + c0, 8), Vo * 8, cudaMemcpyDeviceToHost,
+                                        s->stream));
             } else {
                 LB_TRY(check_launch(s, s->ops().pop_out(s->P, src, s->staging, j, s->stream), "pop_out"));
-                LB_CUDA(cudaMemcpyAsync(f15 + j * V, s->staging, V * 8, cudaMemcpyDeviceToHost, s->stream));
+                LB_CUDA(cudaMemcpyAsync(f15 + j * Vo, s->staging + c0, Vo * 8, cudaMemcpyDeviceToHost, s->stream));
             }
         }
     }
@@ -631,6 +663,8 @@ static int one_step(lbman_solver* s, bool last) {
 int lbman_step(lbman_solver* s, int nsteps) {
     if (!s || nsteps < 0) return fail(LBMAN_ERR_ARG, "bad arguments");
     if (!s->uploaded) return fail(LBMAN_ERR_STATE, "step before upload");
+    if (s->slab)
+        return fail(LBMAN_ERR_STATE, "a slab steps through lbman_qtensor_step and lbman_lbm_step with halo exchanges");
     LB_TRY(set_device(s));
     for (int n = 0; n < nsteps; ++n) LB_TRY(one_step(s, n == nsteps - 1));
     return LBMAN_OK;
@@ -639,10 +673,14 @@ int lbman_step(lbman_solver* s, int nsteps) {
 int lbman_qtensor_step(lbman_solver* s) {
     if (!s) return fail(LBMAN_ERR_ARG, "null solver");
     if (!s->uploaded) return fail(LBMAN_ERR_STATE, "step before upload");
+    if (s->slab && (!s->qu_fresh || s->fout_pending))
+        return fail(LBMAN_ERR_STATE, s->fout_pending ? "exchange LBMAN_HALO_F_OUT after the odd LBM step first"
+                                                     : "exchange LBMAN_HALO_QU before the Q stage of a slab");
     LB_TRY(set_device(s));
     LB_TRY(check_launch(s, s->ops().qforce(s->P, s->shape, s->q[s->qcur], s->u[s->ucur], s->q[1 - s->qcur], s->F, s->stream),
                         "qforce"));
     s->qcur ^= 1;
+    s->qu_fresh = false;
     return LBMAN_OK;
 }
 
@@ -654,6 +692,7 @@ static int ensure_stress(lbman_solver* s) {
 int lbman_qtensor_setup(lbman_solver* s) {
     if (!s) return fail(LBMAN_ERR_ARG, "null solver");
     if (!s->uploaded) return fail(LBMAN_ERR_STATE, "step before upload");
+    if (s->slab) return fail(LBMAN_ERR_UNSUPPORTED, "the two-phase Q stage is not available on slabs");
     LB_TRY(set_device(s));
     LB_TRY(ensure_stress(s));
     const int64_t V = s->P.V;
@@ -667,6 +706,7 @@ int lbman_qtensor_setup(lbman_solver* s) {
 int lbman_active_force(lbman_solver* s) {
     if (!s) return fail(LBMAN_ERR_ARG, "null solver");
     if (!s->uploaded) return fail(LBMAN_ERR_STATE, "step before upload");
+    if (s->slab) return fail(LBMAN_ERR_UNSUPPORTED, "the two-phase Q stage is not available on slabs");
     if (!s->stress) return fail(LBMAN_ERR_STATE, "no stress: call lbman_qtensor_setup or lbman_upload_stress first");
     LB_TRY(set_device(s));
     const int64_t V = s->P.V;
@@ -701,8 +741,16 @@ int lbman_download_stress(lbman_solver* s, double* sigma5, double* tau3) {
 int lbman_lbm_step(lbman_solver* s) {
     if (!s) return fail(LBMAN_ERR_ARG, "null solver");
     if (!s->uploaded) return fail(LBMAN_ERR_STATE, "step before upload");
+    const bool odd = s->fphase == F_SWAP;
+    if (s->slab && (s->fout_pending || (odd && !s->fin_fresh)))
+        return fail(LBMAN_ERR_STATE, s->fout_pending ? "exchange LBMAN_HALO_F_OUT after the odd LBM step first"
+                                                     : "exchange LBMAN_HALO_F_IN before an odd LBM step of a slab");
     LB_TRY(set_device(s));
     LB_TRY(aa_step(s, true));
+    if (s->slab) {
+        s->qu_fresh = s->fin_fresh = false;
+        s->fout_pending = odd;
+    }
     return LBMAN_OK;
 }
 
@@ -723,11 +771,15 @@ int lbman_reduce(lbman_solver* s, int flags, lbman_diag* out) {
         LB_TRY(check_launch(s, o.flow_reduce(s->P, s->rho, s->u[s->ucur], s->upast, s->partials, G, s->stream), "flow_reduce"));
         LB_TRY(check_launch(s, launch_fold(s->partials, G, 8, 1, s->red_dev, s->stream), "fold"));
     }
+    if ((flags & LBMAN_DIAG_ENERGY) && s->slab && !s->qu_fresh)
+        return fail(LBMAN_ERR_STATE, "the free energy of a slab needs a fresh LBMAN_HALO_QU exchange");
     if (flags & LBMAN_DIAG_ENERGY) {
         LB_TRY(check_launch(s, o.energy_reduce(s->P, s->q[s->qcur], s->partials, G, s->stream), "energy_reduce"));
         LB_TRY(check_launch(s, launch_fold(s->partials, G, 1, 0, s->red_dev + 8, s->stream), "fold"));
     }
-    const bool defects = (flags & LBMAN_DIAG_DEFECTS) && s->P.nx >= 2 && s->P.ny >= 2 && s->P.nz >= 2;
+    // a slab's plaquettes across its faces need the neighbour's director:
+    // not counted
+    const bool defects = (flags & LBMAN_DIAG_DEFECTS) && !s->slab && s->P.nx >= 2 && s->P.ny >= 2 && s->P.nz >= 2;
     if (defects) {
         if (!s->dirbuf) LB_CUDA(cudaMalloc(&s->dirbuf, 3 * V * s->rbytes));
         LB_TRY(check_launch(s, o.director(s->P, s->q[s->qcur], nullptr, s->dirbuf, G, s->stream), "director"));
@@ -752,6 +804,7 @@ namespace {
 
 int stats_ready(lbman_solver* s, int nbins) {
     if (!s->uploaded) return fail(LBMAN_ERR_STATE, "statistics before upload");
+    if (s->slab) return fail(LBMAN_ERR_UNSUPPORTED, "statistics of a slab: download the slabs and assemble the box");
     if (nbins < 1 || nbins > lbman::stats::kMaxBins)
         return fail(LBMAN_ERR_ARG, "nbins must be in [1, %d]", lbman::stats::kMaxBins);
     LB_TRY(set_device(s));
@@ -814,6 +867,7 @@ int lbman_defect_lines(lbman_solver* s, lbman_defects* info, double* points, int
                        int64_t* line_offsets, int64_t offsets_cap) {
     if (!s || !info) return fail(LBMAN_ERR_ARG, "null argument");
     if (!s->uploaded) return fail(LBMAN_ERR_STATE, "defect lines before upload");
+    if (s->slab) return fail(LBMAN_ERR_UNSUPPORTED, "defect lines of a slab: download the slabs and assemble the box");
     const int nx = s->P.nx, ny = s->P.ny, nz = s->P.nz;
     if (nx < 2 || ny < 2 || nz < 2) return fail(LBMAN_ERR_ARG, "defect lines need at least 2 cells per side");
     LB_TRY(set_device(s));
@@ -853,6 +907,8 @@ int lbman_set_shape(lbman_solver* s, const lbman_shape* sh) {
     if (sh->kernels != LBMAN_KERNELS_SPLIT && sh->kernels != LBMAN_KERNELS_FUSED &&
         sh->kernels != LBMAN_KERNELS_SPLIT_PAIR)
         return fail(LBMAN_ERR_ARG, "kernels must be LBMAN_KERNELS_SPLIT, LBMAN_KERNELS_FUSED or LBMAN_KERNELS_SPLIT_PAIR");
+    if (s->slab && sh->kernels == LBMAN_KERNELS_FUSED)
+        return fail(LBMAN_ERR_UNSUPPORTED, "slabs step with the in-place organisations");
     QTile t{sh->tile_x, sh->tile_y, sh->zchunk};
     t.pair = sh->kernels == LBMAN_KERNELS_SPLIT_PAIR;
     if (sh->zchunk < -8) return fail(LBMAN_ERR_ARG, "zchunk must be >= -8 (<= 0: balanced schedule)");
@@ -919,22 +975,23 @@ int lbman_autotune(lbman_solver* s, int steps_per_trial, lbman_shape* best, int*
             if (k == LBMAN_KERNELS_SPLIT_PAIR && (s->prec == LBMAN_FP64 || (s->P.nx & 3) != 0)) continue;
             // the fused organisation needs a second population buffer; a box
             // too large for it is tuned over the in-place organisations only
-            if (k == LBMAN_KERNELS_FUSED && ensure_f1(s) != LBMAN_OK) continue;
+            if (k == LBMAN_KERNELS_FUSED && (s->slab || ensure_f1(s) != LBMAN_OK)) continue;
             for (const auto& t : kTileList) {
                 QTile q{t[0], t[1], 1};
                 q.pair = k == LBMAN_KERNELS_SPLIT_PAIR;
                 if (s->ops().qforce_smem(q) == 0) continue;
                 // the balanced one-wave schedule, then fixed chunks around the
                 // default chunk length
-                const int z0 = default_zchunk(s->P.nx, s->P.ny, s->P.nz, t[0], t[1], s->num_sms);
+                const int nzo = s->P.zhi - s->P.zlo;
+                const int z0 = default_zchunk(s->P.nx, s->P.ny, nzo, t[0], t[1], s->num_sms);
                 // plus 32- and 64-plane chunks: many waves of medium marches keep
                 // the blocks of an SM out of step (measured best for the pair
                 // kernel on large boxes)
-                int zs[8] = {0, -2, -3, z0, std::max(4, z0 / 2), std::min(s->P.nz, 2 * z0), 32, 64};
+                int zs[8] = {0, -2, -3, z0, std::max(4, z0 / 2), std::min(nzo, 2 * z0), 32, 64};
                 for (int zi = 0; zi < 8 && status == LBMAN_OK; ++zi) {
                     bool seen = false;
                     for (int zj = 0; zj < zi; ++zj) seen = seen || zs[zj] == zs[zi];
-                    if (seen || (zi >= 6 && zs[zi] >= s->P.nz)) continue;
+                    if (seen || (zi >= 6 && zs[zi] >= nzo)) continue;
                     cur = {k, t[0], t[1], zs[zi], 0, 0.0};
                     if (lbman_set_shape(s, &cur) != LBMAN_OK) continue;
                     if ((status = time_trial(s, steps_per_trial, e0, e1, &cur.ms_per_step)) != LBMAN_OK) break;
@@ -971,6 +1028,234 @@ int lbman_autotune(lbman_solver* s, int steps_per_trial, lbman_shape* best, int*
     lbman_get_shape(s, best);
     best->ms_per_step = win.ms_per_step;
     if (ntrials) *ntrials = count;
+    return LBMAN_OK;
+}
+
+// ---- z-slabs ---------------------------------------------------------------
+
+int lbman_create_slab(const lbman_config* cfg, int nz_global, int z_offset, lbman_solver** out) {
+    if (!cfg || !out) return fail(LBMAN_ERR_ARG, "null argument");
+    *out = nullptr;
+    LB_TRY(validate(*cfg));
+    const int nzl = cfg->nz;
+    if (nzl < 2) return fail(LBMAN_ERR_ARG, "a slab owns at least 2 planes (the Q halo is 2 planes deep)");
+    if (z_offset < 0 || nz_global < nzl || z_offset > nz_global - nzl)
+        return fail(LBMAN_ERR_ARG, "planes [%d, %d) are not inside a box of %d planes", z_offset, z_offset + nzl, nz_global);
+    for (int k = 4; k < 6; ++k)
+        if (cfg->face[k].qbc != LBMAN_Q_PERIODIC || cfg->face[k].ubc != LBMAN_U_PERIODIC)
+            return fail(LBMAN_ERR_UNSUPPORTED, "z-slabs need periodic z faces (Q and velocity)");
+    if (cfg->kernels == LBMAN_KERNELS_FUSED)
+        return fail(LBMAN_ERR_UNSUPPORTED, "slabs step with the in-place organisations (SPLIT or SPLIT_PAIR)");
+    if ((double)cfg->nx * cfg->ny * (nzl + 4) >= 2147483648.0)
+        return fail(LBMAN_ERR_UNSUPPORTED, "a slab with its ghost planes must hold fewer than 2^31 cells");
+    lbman_config c = *cfg;
+    c.nz = nzl + 4;
+    lbman_solver* s = nullptr;
+    LB_TRY(lbman_create(&c, &s));
+    s->slab = true;
+    s->nz_global = nz_global;
+    s->z_offset = z_offset;
+    SimParams& P = s->P;
+    P.zlo = 2;
+    P.zhi = nzl + 2;
+    P.c0 = 2 * P.nxy;
+    P.c1 = (int64_t)(nzl + 2) * P.nxy;
+    P.gbase = (int64_t)(z_offset - 2) * P.nxy;
+    auto bail = [&](int code) {
+        lbman_destroy(s);
+        return code;
+    };
+    const int64_t V = P.V;
+    // ghost planes start finite; the exchanges fill them before any read
+    cudaError_t e = cudaMemsetAsync(s->f[0], 0, 15 * V * s->sbytes, s->stream);
+    for (int b = 0; b < 2 && e == cudaSuccess; ++b) {
+        e = cudaMemsetAsync(s->q[b], 0, 5 * V * s->rbytes, s->stream);
+        if (e == cudaSuccess) e = cudaMemsetAsync(s->u[b], 0, 3 * V * s->rbytes, s->stream);
+    }
+    if (e == cudaSuccess) e = cudaMemsetAsync(s->rho, 0, V * s->rbytes, s->stream);
+    if (e == cudaSuccess) e = cudaMemsetAsync(s->F, 0, 3 * V * s->rbytes, s->stream);
+    if (e == cudaSuccess) e = cudaMalloc(&s->fstage, 10 * P.nxy * s->sbytes);
+    if (e == cudaSuccess) e = cudaEventCreateWithFlags(&s->ev_ready, cudaEventDisableTiming);
+    if (e == cudaSuccess) e = cudaEventCreateWithFlags(&s->ev_done, cudaEventDisableTiming);
+    if (e == cudaSuccess) e = cudaStreamSynchronize(s->stream);
+    if (e != cudaSuccess) return bail(fail(LBMAN_ERR_CUDA, "slab set-up failed: %s", cudaGetErrorString(e)));
+    *out = s;
+    return LBMAN_OK;
+}
+
+int lbman_slab_info(lbman_solver* s, int* nz_global, int* z_offset, int* nz_local) {
+    if (!s) return fail(LBMAN_ERR_ARG, "null solver");
+    const int nzl = s->P.zhi - s->P.zlo;
+    if (nz_global) *nz_global = s->slab ? s->nz_global : nzl;
+    if (z_offset) *z_offset = s->slab ? s->z_offset : 0;
+    if (nz_local) *nz_local = nzl;
+    return LBMAN_OK;
+}
+
+// The slots whose direction crosses the low z face upward (e_z = +1) and the
+// high face downward (e_z = -1), in increasing order.
+static const int kUpSlots[5] = {5, 7, 8, 9, 10};
+static const int kDownSlots[5] = {6, 11, 12, 13, 14};
+
+int lbman_halo_plan(int nz_local, int phase, lbman_halo_span send[2][LBMAN_HALO_MAX_SPANS],
+                    lbman_halo_span recv[2][LBMAN_HALO_MAX_SPANS], int* n) {
+    if (!send || !recv || !n) return fail(LBMAN_ERR_ARG, "null argument");
+    if (nz_local < 2) return fail(LBMAN_ERR_ARG, "a slab owns at least 2 planes");
+    auto span = [](int field, int comp, int plane, int planes) { return lbman_halo_span{field, comp, plane, planes}; };
+    if (phase == LBMAN_HALO_QU) {
+        // owned -> ghost, 2 planes: the Q+force kernel reads Q and u up to 2
+        // planes beyond the owned ones
+        *n = 8;
+        for (int k = 0; k < 8; ++k) {
+            const int field = k < 5 ? LBMAN_FIELD_Q : LBMAN_FIELD_U, comp = k < 5 ? k : k - 5;
+            send[0][k] = span(field, comp, 0, 2);
+            send[1][k] = span(field, comp, nz_local - 2, 2);
+            recv[0][k] = span(field, comp, -2, 2);
+            recv[1][k] = span(field, comp, nz_local, 2);
+        }
+    } else if (phase == LBMAN_HALO_F_IN) {
+        // before an odd in-place step: a boundary cell gathers f*_j of the
+        // neighbour's boundary plane from slot opp(j) there, i.e. the slots
+        // crossing the face towards the neighbour
+        *n = 5;
+        for (int k = 0; k < 5; ++k) {
+            send[0][k] = span(LBMAN_FIELD_F, kUpSlots[k], 0, 1);
+            recv[1][k] = span(LBMAN_FIELD_F, kUpSlots[k], nz_local, 1);
+            send[1][k] = span(LBMAN_FIELD_F, kDownSlots[k], nz_local - 1, 1);
+            recv[0][k] = span(LBMAN_FIELD_F, kDownSlots[k], -1, 1);
+        }
+    } else if (phase == LBMAN_HALO_F_OUT) {
+        // after it: those slots, rewritten by this slab's boundary cells,
+        // go back to the neighbour's boundary plane (via its staging area)
+        *n = 5;
+        for (int k = 0; k < 5; ++k) {
+            send[0][k] = span(LBMAN_FIELD_F, kDownSlots[k], -1, 1);
+            recv[1][k] = span(LBMAN_FIELD_FSTAGE, k, 1, 1);
+            send[1][k] = span(LBMAN_FIELD_F, kUpSlots[k], nz_local, 1);
+            recv[0][k] = span(LBMAN_FIELD_FSTAGE, k, 0, 1);
+        }
+    } else {
+        return fail(LBMAN_ERR_ARG, "bad halo phase %d", phase);
+    }
+    return LBMAN_OK;
+}
+
+static void* span_ptr(lbman_solver* s, const lbman_halo_span& sp) {
+    const SimParams& P = s->P;
+    const int64_t plane = (int64_t)(P.zlo + sp.plane) * P.nxy;
+    switch (sp.field) {
+        case LBMAN_FIELD_Q: return vptr(s->q[s->qcur], sp.comp * P.V + plane, s->rbytes);
+        case LBMAN_FIELD_U: return vptr(s->u[s->ucur], sp.comp * P.V + plane, s->rbytes);
+        case LBMAN_FIELD_F: return vptr(s->f[s->fcur], sp.comp * P.V + plane, s->sbytes);
+        default: return vptr(s->fstage, (int64_t)(sp.plane * 5 + sp.comp) * P.nxy, s->sbytes);
+    }
+}
+
+// Does the phase move anything now: the population halos only around odd
+// in-place steps.
+static bool halo_active(const lbman_solver* s, int phase) {
+    if (phase == LBMAN_HALO_F_IN) return s->fphase == F_SWAP;
+    if (phase == LBMAN_HALO_F_OUT) return s->fout_pending;
+    return true;
+}
+
+int lbman_halo_spans(lbman_solver* s, int phase, void* send[2][LBMAN_HALO_MAX_SPANS],
+                     void* recv[2][LBMAN_HALO_MAX_SPANS], size_t* span_bytes, int* n) {
+    if (!s || !send || !recv || !span_bytes || !n) return fail(LBMAN_ERR_ARG, "null argument");
+    if (!s->slab) return fail(LBMAN_ERR_STATE, "not a slab (lbman_create_slab)");
+    if (!s->uploaded) return fail(LBMAN_ERR_STATE, "exchange before upload");
+    lbman_halo_span ps[2][LBMAN_HALO_MAX_SPANS], pr[2][LBMAN_HALO_MAX_SPANS];
+    int cnt = 0;
+    LB_TRY(lbman_halo_plan(s->P.zhi - s->P.zlo, phase, ps, pr, &cnt));
+    *n = halo_active(s, phase) ? cnt : 0;
+    *span_bytes = (size_t)(ps[0][0].planes * s->P.nxy) * (phase == LBMAN_HALO_QU ? s->rbytes : s->sbytes);
+    for (int f = 0; f < 2; ++f)
+        for (int k = 0; k < *n; ++k) {
+            send[f][k] = span_ptr(s, ps[f][k]);
+            recv[f][k] = span_ptr(s, pr[f][k]);
+        }
+    return LBMAN_OK;
+}
+
+int lbman_halo_done(lbman_solver* s, int phase) {
+    if (!s) return fail(LBMAN_ERR_ARG, "null solver");
+    if (!s->slab) return fail(LBMAN_ERR_STATE, "not a slab (lbman_create_slab)");
+    if (phase == LBMAN_HALO_QU) {
+        s->qu_fresh = true;
+    } else if (phase == LBMAN_HALO_F_IN) {
+        if (s->fphase == F_SWAP) s->fin_fresh = true;
+    } else if (phase == LBMAN_HALO_F_OUT) {
+        if (s->fout_pending) {
+            LB_TRY(set_device(s));
+            const int64_t nxy = s->P.nxy;
+            for (int face = 0; face < 2; ++face)
+                LB_TRY(check_launch(s, s->ops().halo_merge(s->P, s->f[s->fcur], vptr(s->fstage, face * 5 * nxy, s->sbytes),
+                                                           face, s->stream),
+                                    "halo_merge"));
+            s->fout_pending = false;
+        }
+    } else {
+        return fail(LBMAN_ERR_ARG, "bad halo phase %d", phase);
+    }
+    return LBMAN_OK;
+}
+
+int lbman_slab_exchange(lbman_solver* const* slabs, int nslabs, int phase) {
+    if (!slabs || nslabs < 1) return fail(LBMAN_ERR_ARG, "no slabs");
+    const int n = nslabs;
+    struct Spans {
+        void* send[2][LBMAN_HALO_MAX_SPANS];
+        void* recv[2][LBMAN_HALO_MAX_SPANS];
+        size_t bytes = 0;
+        int n = 0;
+    };
+    std::vector<Spans> sp((size_t)n);
+    int zsum = 0;
+    for (int i = 0; i < n; ++i) {
+        lbman_solver* s = slabs[i];
+        if (!s || !s->slab) return fail(LBMAN_ERR_ARG, "slab %d is not a slab handle", i);
+        if (s->z_offset != zsum || s->nz_global != slabs[0]->nz_global || s->P.nxy != slabs[0]->P.nxy ||
+            s->prec != slabs[0]->prec)
+            return fail(LBMAN_ERR_ARG, "slabs must tile the box in z order with one shape and precision");
+        zsum += s->P.zhi - s->P.zlo;
+        LB_TRY(lbman_halo_spans(s, phase, sp[i].send, sp[i].recv, &sp[i].bytes, &sp[i].n));
+        if (sp[i].n != sp[0].n) return fail(LBMAN_ERR_STATE, "slabs are at different steps");
+    }
+    if (zsum != slabs[0]->nz_global) return fail(LBMAN_ERR_ARG, "the slabs cover %d of %d planes", zsum, slabs[0]->nz_global);
+    if (sp[0].n > 0) {
+        for (int i = 0; i < n; ++i) {
+            LB_TRY(set_device(slabs[i]));
+            LB_CUDA(cudaEventRecord(slabs[i]->ev_ready, slabs[i]->stream));
+        }
+        for (int j = 0; j < n; ++j) {
+            lbman_solver* r = slabs[j];
+            const int lo = (j + n - 1) % n, hi = (j + 1) % n;
+            LB_TRY(set_device(r));
+            for (int nb : {lo, hi}) {
+                if (slabs[nb]->device != r->device) {
+                    cudaError_t e = cudaDeviceEnablePeerAccess(slabs[nb]->device, 0);
+                    if (e == cudaErrorPeerAccessAlreadyEnabled) cudaGetLastError();
+                    else if (e != cudaSuccess) cudaGetLastError();  // copies are staged by the driver instead
+                }
+                LB_CUDA(cudaStreamWaitEvent(r->stream, slabs[nb]->ev_ready, 0));
+            }
+            // the low ghosts come from the lower slab's sends across its high
+            // face, the high ghosts from the upper slab's sends across its low face
+            for (int k = 0; k < sp[j].n; ++k) {
+                LB_CUDA(cudaMemcpyAsync(sp[j].recv[0][k], sp[lo].send[1][k], sp[j].bytes, cudaMemcpyDefault, r->stream));
+                LB_CUDA(cudaMemcpyAsync(sp[j].recv[1][k], sp[hi].send[0][k], sp[j].bytes, cudaMemcpyDefault, r->stream));
+            }
+            LB_CUDA(cudaEventRecord(r->ev_done, r->stream));
+        }
+        // a slab's next kernel may overwrite what its neighbours copy out
+        for (int i = 0; i < n; ++i) {
+            lbman_solver* s = slabs[i];
+            LB_TRY(set_device(s));
+            LB_CUDA(cudaStreamWaitEvent(s->stream, slabs[(i + n - 1) % n]->ev_done, 0));
+            LB_CUDA(cudaStreamWaitEvent(s->stream, slabs[(i + 1) % n]->ev_done, 0));
+        }
+    }
+    for (int i = 0; i < n; ++i) LB_TRY(lbman_halo_done(slabs[i], phase));
     return LBMAN_OK;
 }
 

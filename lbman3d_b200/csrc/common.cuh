@@ -35,6 +35,13 @@ struct Phys {
 struct SimParams {
     int nx, ny, nz;
     int64_t V, nxy;
+    // The planes [zlo, zhi) and cells [c0, c1) a step updates: the whole box,
+    // or the owned planes of a z-slab allocated with ghost planes on both
+    // sides (the z axis is then periodic in the kernels' view and never
+    // wraps, because every neighbour of an owned plane is allocated).  gbase
+    // maps a cell index to its index in the whole box.
+    int zlo, zhi;
+    int64_t c0, c1, gbase;
     double DT, kDensity, L, A, B, C, LAMBDA, GAMMA, ALPHA, MU;
     double omega, omega_prime, omega_forcing;
     int upwind;

@@ -26,19 +26,20 @@ template <class R>
 __global__ void __launch_bounds__(256) seeded_init_kernel(SimParams P, uint64_t key, double S0, double sigma,
                                                           R* __restrict__ rho, R* __restrict__ u,
                                                           R* __restrict__ q, R* __restrict__ F) {
-    const int64_t c = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
-    if (c >= P.V) return;
+    const int64_t c = P.c0 + (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (c >= P.c1) return;
     const int64_t V = P.V;
+    const uint64_t gc = (uint64_t)(c + P.gbase);  // index in the whole box
     const double two_pi = 6.283185307179586476925286766559;
-    const double ct = 2.0 * uniform01(key, (uint64_t)c, 0) - 1.0;
-    const double ph = two_pi * uniform01(key, (uint64_t)c, 1);
+    const double ct = 2.0 * uniform01(key, gc, 0) - 1.0;
+    const double ph = two_pi * uniform01(key, gc, 1);
     const double st = sqrt(fmax(0.0, 1.0 - ct * ct));
     const double n0 = st * cos(ph), n1 = st * sin(ph), n2 = ct;
     double g[6];
 #pragma unroll
     for (int k = 0; k < 3; ++k) {
-        const double r = sqrt(-2.0 * log(uniform01(key, (uint64_t)c, 2 + 2 * k)));
-        const double t = two_pi * uniform01(key, (uint64_t)c, 3 + 2 * k);
+        const double r = sqrt(-2.0 * log(uniform01(key, gc, 2 + 2 * k)));
+        const double t = two_pi * uniform01(key, gc, 3 + 2 * k);
         g[2 * k] = r * cos(t);
         g[2 * k + 1] = r * sin(t);
     }

@@ -21,7 +21,7 @@ inline unsigned blocks_for(int64_t n, int threads) { return (unsigned)((n + thre
 
 inline dim3 qgrid(const SimParams& P, int tcx, int tcy, int zc) {
     return dim3((unsigned)((P.nx + tcx - 1) / tcx), (unsigned)((P.ny + tcy - 1) / tcy),
-                (unsigned)((P.nz + zc - 1) / zc));
+                (unsigned)((P.zhi - P.zlo + zc - 1) / zc));
 }
 
 constexpr size_t kMaxSmem = 227 * 1024;
@@ -109,7 +109,7 @@ int resident_blocks(int threads, size_t smem) {
 template <class TL, auto Kern>
 dim3 march_grid(const SimParams& P, const LaunchShape& S, size_t smem) {
     if (S.tile.zc > 0) return qgrid(P, TL::TCX, TL::TCY, S.tile.zc);
-    const int64_t units = (int64_t)((P.nx + TL::TCX - 1) / TL::TCX) * ((P.ny + TL::TCY - 1) / TL::TCY) * P.nz;
+    const int64_t units = (int64_t)((P.nx + TL::TCX - 1) / TL::TCX) * ((P.ny + TL::TCY - 1) / TL::TCY) * (P.zhi - P.zlo);
     const int64_t waves = std::max(1, -S.tile.zc);
     const int64_t grid = waves * resident_blocks<Kern>(TL::NT, smem) * S.num_sms;
     return dim3((unsigned)std::max<int64_t>(1, std::min(units, grid)));
@@ -247,7 +247,7 @@ template <class R, class S, bool DEV>
 cudaError_t lbm_aa(const SimParams& P, bool odd, bool wr, void* f, const void* F, void* rho, void* uout,
                    cudaStream_t st) {
     const FastDiv dnx = make_fastdiv((uint32_t)P.nx), dnxy = make_fastdiv((uint32_t)P.nxy);
-    const unsigned nb = blocks_for(P.V, 256);
+    const unsigned nb = blocks_for(P.c1 - P.c0, 256);
     auto launch = [&](auto kern) {
         kern<<<nb, 256, 0, st>>>(P, dnx, dnxy, (S*)f, (const R*)F, (R*)rho, (R*)uout, wr ? 1 : 0);
     };
@@ -279,6 +279,12 @@ cudaError_t aa_pop_out(const SimParams& P, const void* f, const void* rho, doubl
     const FastDiv dnx = make_fastdiv((uint32_t)P.nx), dnxy = make_fastdiv((uint32_t)P.nxy);
     aa_pop_out_kernel<R, S, DEV><<<blocks_for(P.V, 256), 256, 0, st>>>(P, dnx, dnxy, (const S*)f, (const R*)rho, dst,
                                                                       dir);
+    return cudaGetLastError();
+}
+
+template <class S>
+cudaError_t halo_merge(const SimParams& P, void* f, const void* stage, int face, cudaStream_t st) {
+    halo_merge_kernel<S><<<blocks_for(P.nxy, 256), 256, 0, st>>>(P, (S*)f, (const S*)stage, face);
     return cudaGetLastError();
 }
 
@@ -320,18 +326,21 @@ __global__ void from_storage_kernel(const T* __restrict__ src, double* __restric
     if (i < n) dst[i] = from_s(src + i) + off;
 }
 
-// Populations of direction dir: host f_i <-> stored value (deviation form
-// subtracts w_i rho0).
+// Populations of direction dir over the cells [c0, c1): host f_i <-> stored
+// value (deviation form subtracts w_i rho0); src / dst hold whole-allocation
+// arrays.
 template <class S, bool DEV>
 cudaError_t pop_in(const SimParams& P, const double* src, void* dst, int dir, cudaStream_t st) {
     const double off = DEV ? w_<double>(dir) * P.kDensity : 0.0;
-    to_storage_kernel<S><<<blocks_for(P.V, 256), 256, 0, st>>>(src, (S*)dst + (int64_t)dir * P.V, P.V, off);
+    to_storage_kernel<S><<<blocks_for(P.c1 - P.c0, 256), 256, 0, st>>>(src + P.c0, (S*)dst + (int64_t)dir * P.V + P.c0,
+                                                                       P.c1 - P.c0, off);
     return cudaGetLastError();
 }
 template <class S, bool DEV>
 cudaError_t pop_out(const SimParams& P, const void* src, double* dst, int dir, cudaStream_t st) {
     const double off = DEV ? w_<double>(dir) * P.kDensity : 0.0;
-    from_storage_kernel<S><<<blocks_for(P.V, 256), 256, 0, st>>>((const S*)src + (int64_t)dir * P.V, dst, P.V, off);
+    from_storage_kernel<S><<<blocks_for(P.c1 - P.c0, 256), 256, 0, st>>>((const S*)src + (int64_t)dir * P.V + P.c0,
+                                                                         dst + P.c0, P.c1 - P.c0, off);
     return cudaGetLastError();
 }
 template <class R>
@@ -377,7 +386,7 @@ template <class R>
 cudaError_t seeded_init(const SimParams& P, uint64_t seed, double S0, double sigma, void* rho, void* u, void* q,
                         void* F, cudaStream_t st) {
     const uint64_t key = splitmix64(seed ^ 0x5851f42d4c957f2dULL);
-    seeded_init_kernel<R><<<blocks_for(P.V, 256), 256, 0, st>>>(P, key, S0, sigma, (R*)rho, (R*)u, (R*)q, (R*)F);
+    seeded_init_kernel<R><<<blocks_for(P.c1 - P.c0, 256), 256, 0, st>>>(P, key, S0, sigma, (R*)rho, (R*)u, (R*)q, (R*)F);
     return cudaGetLastError();
 }
 
@@ -468,6 +477,10 @@ cudaError_t prepare(size_t max_smem) {
     }                                                                                                   \
     cudaError_t launch_swap_pairs_##SUF(const SimParams& P, void* f, cudaStream_t st) {                \
         return impl::swap_pairs<S>(P, f, st);                                                           \
+    }                                                                                                   \
+    cudaError_t launch_halo_merge_##SUF(const SimParams& P, void* f, const void* stage, int face,       \
+                                        cudaStream_t st) {                                              \
+        return impl::halo_merge<S>(P, f, stage, face, st);                                              \
     }                                                                                                   \
     cudaError_t launch_feq_init_##SUF(const SimParams& P, const void* rho, const void* u, void* f,     \
                                       cudaStream_t st) {                                               \

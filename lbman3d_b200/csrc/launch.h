@@ -35,6 +35,8 @@ struct LaunchShape {
     cudaError_t launch_aa_pop_out_##SUF(const SimParams& P, const void* f, const void* rho, double* dst, \
                                         int dir, cudaStream_t st);                                     \
     cudaError_t launch_swap_pairs_##SUF(const SimParams& P, void* f, cudaStream_t st);                 \
+    cudaError_t launch_halo_merge_##SUF(const SimParams& P, void* f, const void* stage, int face,      \
+                                        cudaStream_t st);                                              \
     cudaError_t launch_feq_init_##SUF(const SimParams& P, const void* rho, const void* u, void* f,     \
                                       cudaStream_t st);                                                \
     cudaError_t launch_pop_in_##SUF(const SimParams& P, const double* src, void* dst, int dir,         \

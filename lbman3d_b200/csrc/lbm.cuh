@@ -405,8 +405,8 @@ template <class R, class S, bool DEV, int WM, class I>
 __global__ void __launch_bounds__(256, lbm_min_blocks<R, S, WM != 0>())
     lbm_aa_even_kernel(const __grid_constant__ SimParams P, FastDiv dnx, FastDiv dnxy, S* F, const R* __restrict__ Fb,
                        R* __restrict__ rho_buf, R* __restrict__ uout, int write_rho_all) {
-    const I c = (I)blockIdx.x * (I)blockDim.x + (I)threadIdx.x;
-    if (c >= (I)P.V) return;
+    const I c = (I)P.c0 + (I)blockIdx.x * (I)blockDim.x + (I)threadIdx.x;
+    if (c >= (I)P.c1) return;
     const I V = (I)P.V;
     const Phys<R>& K = phys_ref<R>(P);
     S raw[15];
@@ -438,8 +438,8 @@ template <class R, class S, bool DEV, int WM, class I>
 __global__ void __launch_bounds__(256, lbm_min_blocks<R, S, WM != 0>())
     lbm_aa_odd_kernel(const __grid_constant__ SimParams P, FastDiv dnx, FastDiv dnxy, S* F, const R* __restrict__ Fb,
                       R* __restrict__ rho_buf, R* __restrict__ uout, int write_rho_all) {
-    const I c = (I)blockIdx.x * (I)blockDim.x + (I)threadIdx.x;
-    if (c >= (I)P.V) return;
+    const I c = (I)P.c0 + (I)blockIdx.x * (I)blockDim.x + (I)threadIdx.x;
+    if (c >= (I)P.c1) return;
     const I V = (I)P.V;
     const Phys<R>& K = phys_ref<R>(P);
     CellPos q;
@@ -548,6 +548,34 @@ __global__ void __launch_bounds__(256) aa_pop_out_kernel(const __grid_constant__
     q.x = (int)(r - (uint32_t)q.y * (uint32_t)P.nx);
     const R v = aa_pre_population<R, S>(P, phys_ref<R>(P), F, c, q, dir, rho_buf);
     dst[c] = (double)v + (DEV ? w_<double>(dir) * P.kDensity : 0.0);
+}
+
+// Merge of the populations a neighbouring z-slab scattered across face
+// `face` (0: low, 1: high) in an odd in-place step into this slab's owned
+// boundary plane (zlo or zhi - 1).  They arrive staged as 5 planes, the
+// slots k crossing that face (e_z = +1 at the low face, -1 at the high face)
+// in increasing order.  Slot k of cell c holds f*_k of the source c - e_k;
+// where that source lies beyond an x or y wall, the neighbour has no thread
+// for it and this cell's own wall rule wrote the slot in the same step, so
+// the slot is kept (the reference's unpack skip rule,
+// src/mpi/halo_exchange_lbm.h SkipUnpackXY).
+template <class S>
+__global__ void __launch_bounds__(256) halo_merge_kernel(const __grid_constant__ SimParams P, S* F,
+                                                         const S* __restrict__ stage, int face) {
+    const int64_t t = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (t >= P.nxy) return;
+    const int y = (int)(t / P.nx), x = (int)(t - (int64_t)y * P.nx);
+    const int64_t c = (int64_t)(face == 0 ? P.zlo : P.zhi - 1) * P.nxy + t;
+    const int ez = face == 0 ? 1 : -1;
+    int n = 0;
+#pragma unroll
+    for (int k = 1; k < 15; ++k) {
+        if (ez_(k) != ez) continue;
+        const bool cx = ex_(k) != 0 && !P.uper[0] && ((ex_(k) > 0 && x == 0) || (ex_(k) < 0 && x == P.nx - 1));
+        const bool cy = ey_(k) != 0 && !P.uper[2] && ((ey_(k) > 0 && y == 0) || (ey_(k) < 0 && y == P.ny - 1));
+        if (!cx && !cy) F[k * P.V + c] = stage[n * P.nxy + t];
+        ++n;
+    }
 }
 
 // In-place exchange of the direction slots j and opp(j) of every cell:

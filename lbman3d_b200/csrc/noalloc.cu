@@ -75,6 +75,8 @@ extern "C" int lbman_flow_reduce_noalloc(int64_t ncells, int precision, const vo
     SimParams P;
     std::memset(&P, 0, sizeof(P));
     P.V = ncells;
+    P.c0 = 0;
+    P.c1 = ncells;  // the reduction's cell range
     const int G = (int)((ncells + kRedThreads - 1) / kRedThreads < kMaxBlocks
                             ? (ncells + kRedThreads - 1) / kRedThreads
                             : kMaxBlocks);

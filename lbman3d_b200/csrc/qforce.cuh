@@ -511,20 +511,21 @@ template <class TL, class R, bool UPWIND, class OutFn>
 __device__ __forceinline__ void qf_run(const SimParams& P, int zc_len, const R* __restrict__ qin,
                                        const R* __restrict__ uin, R* smem, OutFn&& out) {
     if (zc_len > 0) {
-        const int z0 = blockIdx.z * zc_len;
-        if (z0 >= P.nz) return;
-        qf_march<TL, R, UPWIND>(P, blockIdx.x * TL::TCX, blockIdx.y * TL::TCY, z0, min(z0 + zc_len, P.nz), qin,
+        const int z0 = P.zlo + (int)blockIdx.z * zc_len;
+        if (z0 >= P.zhi) return;
+        qf_march<TL, R, UPWIND>(P, blockIdx.x * TL::TCX, blockIdx.y * TL::TCY, z0, min(z0 + zc_len, P.zhi), qin,
                                 uin, smem, out);
         return;
     }
     const int cx = (P.nx + TL::TCX - 1) / TL::TCX, cy = (P.ny + TL::TCY - 1) / TL::TCY;
-    const int64_t W = (int64_t)cx * cy * P.nz;
+    const int nzo = P.zhi - P.zlo;
+    const int64_t W = (int64_t)cx * cy * nzo;
     int64_t w = W * blockIdx.x / gridDim.x;
     const int64_t w1 = W * (blockIdx.x + 1) / gridDim.x;
     while (w < w1) {
-        const int64_t col = w / P.nz;
-        const int z0 = (int)(w - col * P.nz);
-        const int z1 = (int)min((int64_t)P.nz, z0 + (w1 - w));
+        const int64_t col = w / nzo;
+        const int z0 = P.zlo + (int)(w - col * nzo);
+        const int z1 = (int)min((int64_t)P.zhi, z0 + (w1 - w));
         const int by = (int)(col / cx), bx = (int)(col - (int64_t)by * cx);
         qf_march<TL, R, UPWIND>(P, bx * TL::TCX, by * TL::TCY, z0, z1, qin, uin, smem, out);
         __syncthreads();  // the staging rings are reused by the next segment

@@ -57,7 +57,8 @@ __global__ void __launch_bounds__(kRedThreads) flow_reduce_kernel(SimParams P, c
                                                                   double* __restrict__ partials) {
     const int64_t V = P.V;
     double v[kFlowQ] = {0, 0, 0, 0, 0, 0, 0, 0};
-    for (int64_t c = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; c < V; c += (int64_t)gridDim.x * blockDim.x) {
+    for (int64_t c = P.c0 + (int64_t)blockIdx.x * blockDim.x + threadIdx.x; c < P.c1;
+         c += (int64_t)gridDim.x * blockDim.x) {
         const double r = (double)rho[c];
         const double ux = (double)u[c], uy = (double)u[V + c], uz = (double)u[2 * V + c];
         const double px = (double)upast[c], py = (double)upast[V + c], pz = (double)upast[2 * V + c];
@@ -84,7 +85,8 @@ __global__ void __launch_bounds__(kRedThreads) energy_reduce_kernel(SimParams P,
     const int64_t V = P.V;
     const int nx = P.nx, ny = P.ny, nz = P.nz;
     double v[1] = {0.0};
-    for (int64_t c = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; c < V; c += (int64_t)gridDim.x * blockDim.x) {
+    for (int64_t c = P.c0 + (int64_t)blockIdx.x * blockDim.x + threadIdx.x; c < P.c1;
+         c += (int64_t)gridDim.x * blockDim.x) {
         const int z = (int)(c / P.nxy);
         const int rr = (int)(c - (int64_t)z * P.nxy);
         const int y = rr / nx, x = rr - y * nx;
