@@ -431,6 +431,77 @@ def side_workloads(names, device, stream, steps=2000):
     return out
 
 
+def halo_bytes_per_step(nx, ny, precision):
+    """Bytes one slab sends per step: the Q/u halo (2 faces x 8 components x
+    2 planes) every step, the population halos (2 faces x 5 slots, in and
+    out) every other step."""
+    rb = 8 if precision == "fp64" else 4
+    sb = {"fp64": 8, "fp32": 4, "fp16": 2}[precision]
+    return nx * ny * (2 * 8 * 2 * rb + 2 * 5 * sb)
+
+
+def make_slabs(workload, precision, device, kernels, tile, nslabs):
+    import lbman3d_b200 as L
+    nx, ny, nz, bc, alpha, _ = WORKLOADS[workload]
+    p = L.Params(nx=nx, ny=ny, nz=nz, ALPHA=alpha)
+    prec = {"fp64": L.Precision.FP64, "fp32": L.Precision.FP32, "fp16": L.Precision.FP16}[precision]
+    return L.SlabBox(p, bc_for(bc), prec, nslabs=nslabs, kernels=kernels, devices=(device,), tile=tile), p
+
+
+def slab_split(workload, precision, device, stream, kernels, tile, nslabs=2, steps=40, warmup=4):
+    """The box as nslabs z-slabs on this one GPU, exchanging through
+    lbman_slab_exchange on one stream: the cost of the decomposition's ghost
+    planes, exchanges and extra launches, against the single box."""
+    import torch
+    sb, p = make_slabs(workload, precision, device, kernels, tile, nslabs)
+    try:
+        for s in sb.slabs:
+            s.set_stream(stream.cuda_stream)
+        sb.init_seeded(SEED, S0, SIGMA)
+        sb.step(warmup)
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record(stream)
+        sb.step(steps)
+        e1.record(stream)
+        e1.synchronize()
+        ms = e0.elapsed_time(e1)
+    finally:
+        sb.close()
+    return {"slabs": nslabs, "value": p.V * steps / (ms * 1e3), "unit": "MLUPS", "steps": steps,
+            "ms_per_step": ms / steps, "halo_bytes_per_slab_step": halo_bytes_per_step(p.nx, p.ny, precision)}
+
+
+def time_slab_ranks(a, workload, local, stream):
+    """Strong scaling (--decomp slab): the box split into one z-slab per rank,
+    exchanging over NCCL point-to-point operations (DistributedSlab)."""
+    import torch
+    import lbman3d_b200 as L
+    nx, ny, nz, bc, alpha, _ = WORKLOADS[workload]
+    p = L.Params(nx=nx, ny=ny, nz=nz, ALPHA=alpha)
+    prec = {"fp64": L.Precision.FP64, "fp32": L.Precision.FP32, "fp16": L.Precision.FP16}[a.precision]
+    kern = {"auto": L._native.KERNELS_AUTO, "split": L._native.KERNELS_SPLIT,
+            "pair": L._native.KERNELS_SPLIT_PAIR}[a.kernels]
+    tile = tuple(int(v) for v in a.tile.split(",")) if a.tile else None
+    with torch.cuda.stream(stream):
+        ds = L.DistributedSlab(p, bc_for(bc), prec, kern, tile=tile)
+        try:
+            ds.slab.init_seeded(SEED, S0, SIGMA)
+            if a.kernels == "auto" and not tile:  # per slab; restores the state it advances
+                ds.slab.autotune(steps_per_trial=8)
+            ds.step(max(a.warmup, 3))
+            l0 = ds.slab.launch_count()
+            e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            e0.record(stream)
+            ds.step(a.steps)
+            e1.record(stream)
+            e1.synchronize()
+            ms, launches = e0.elapsed_time(e1), ds.slab.launch_count() - l0
+            d = ds.reduce(L._native.DIAG_FLOW)
+        finally:
+            ds.close()
+    return ms, launches, d, halo_bytes_per_step(nx, ny, a.precision)
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -444,6 +515,8 @@ def main():
     ap.add_argument("--no-extras", action="store_true", help="skip e2e, cpu baseline and variants")
     ap.add_argument("--kernels", default="auto", choices=["auto", "fused", "split", "pair"])
     ap.add_argument("--tile", default=None, help="tcx,tcy[,zchunk] of the z-marching kernels")
+    ap.add_argument("--decomp", default="replicas", choices=["replicas", "slab"],
+                    help="N > 1: one box per GPU (weak scaling) or one box split into z-slabs (strong)")
     a = ap.parse_args()
 
     rank = int(os.environ.get("RANK", "0"))
@@ -480,6 +553,33 @@ def main():
         dist.init_process_group("nccl", init_method="env://", timeout=datetime.timedelta(seconds=300))
     torch.cuda.set_device(local)
     stream = torch.cuda.Stream(device=local)
+
+    if a.decomp == "slab":
+        config["parallelism"] = f"z-slabs x{world}"
+        if world > 1:
+            dist.barrier()
+        torch.cuda.synchronize()
+        with ClockSampler(local) as clk:
+            ms, launches, diag, hb = time_slab_ranks(a, a.workload, local, stream)
+        ms = reduce_max(ms, world, "cuda")
+        peak, peak_kind = measured_peaks()
+        bpc = BYTES_PER_CELL[a.precision]
+        step_achieved = bpc * V / (ms / a.steps * 1e-3) / 1e9
+        line = {"metric": "MLUPS", "value": V * a.steps / (ms * 1e3), "unit": "MLUPS", "n_gpus": world,
+                "steps": a.steps, "warmup": max(a.warmup, 3), "ms_per_step": ms / a.steps, "higher_is_better": True,
+                "scaling": "strong", "vs_baseline": None,
+                "dtype": {"fp32": "f32", "fp64": "f64", "fp16": "f32 (f16 storage)"}[a.precision],
+                "data": "synthetic", "config": config, "gpu_launches": launches,
+                "roofline": {"bound": "hbm", "achieved": step_achieved, "peak": peak * world, "unit": "GB/s",
+                             "frac": step_achieved / (peak * world), "traffic": None, "peak_kind": peak_kind,
+                             "kernel": "step (all slabs)", "step_bytes_per_cell": bpc},
+                "halo_bytes_per_rank_step": hb, "mass": diag["mass"], "clocks": clk.summary()}
+        if rank == 0:
+            print(json.dumps(line), flush=True)
+        if world > 1:
+            dist.barrier()
+            dist.destroy_process_group()
+        return
 
     tile = tuple(int(v) for v in a.tile.split(",")) if a.tile else None
     sim, p = make_sim(a.workload, a.precision, local, a.kernels, tile)
@@ -548,6 +648,10 @@ def main():
         line["other_workloads"] = side_workloads([w for w in ("slit64", "channel20") if w != a.workload], local,
                                                  stream)
         line["ensemble"] = ensemble_vs_sequential(local, stream)
+        kern_id = {"split": 1, "split_pair": 3}.get(config["kernels"], 1)
+        line["slab_split"] = slab_split(a.workload, a.precision, local, stream, kern_id, tuple(config["tile"]))
+        line["slab_split"]["vs_single_box"] = line["slab_split"]["value"] / mlups
+        torch.cuda.empty_cache()
         try:
             r = reference_cpu(a.workload, ref_sample_steps(V, a.steps), 1)
             line["cpu_baseline"] = {k: v for k, v in r.items() if k != "ms_step"}

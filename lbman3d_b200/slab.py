@@ -102,12 +102,6 @@ class Slab(Simulation):
     def halo_done(self, phase: int):
         N.check(N.lib().lbman_halo_done(self._h, int(phase)))
 
-    def set_stream(self, cuda_stream: int):
-        N.check(N.lib().lbman_set_stream(self._h, C.c_void_p(int(cuda_stream))))
-
-    def synchronize(self):
-        N.check(N.lib().lbman_synchronize(self._h))
-
 
 def _split_field(a: np.ndarray, ncomp: int, nxy: int, parts):
     """Owned-plane blocks of a whole-box field of ncomp components."""
@@ -254,7 +248,10 @@ class DistributedSlab:
         import torch
         import torch.distributed as dist
         self.dist, self.group = dist, group
-        self.rank, self.world = dist.get_rank(group), dist.get_world_size(group)
+        if dist.is_available() and dist.is_initialized():
+            self.rank, self.world = dist.get_rank(group), dist.get_world_size(group)
+        else:  # one process: the whole box in one slab
+            self.rank, self.world = 0, 1
         self.device = torch.cuda.current_device()
         z0, n = split_planes(params.nz, self.world)[self.rank]
         self.slab = Slab(params, bc, precision, kernels, z0, n, self.device, tile)
@@ -290,8 +287,9 @@ class DistributedSlab:
         keys = [k for k in d if k not in ("umax2", "nan_detected", "defect_faces")]
         s = torch.tensor([d[k] for k in keys], dtype=torch.float64, device=self.device)
         m = torch.tensor([d["umax2"], float(d["nan_detected"])], dtype=torch.float64, device=self.device)
-        self.dist.all_reduce(s, group=self.group)
-        self.dist.all_reduce(m, op=self.dist.ReduceOp.MAX, group=self.group)
+        if self.world > 1:
+            self.dist.all_reduce(s, group=self.group)
+            self.dist.all_reduce(m, op=self.dist.ReduceOp.MAX, group=self.group)
         out = dict(zip(keys, s.tolist()))
         out["umax2"], out["nan_detected"], out["defect_faces"] = m[0].item(), int(m[1].item()), -1
         return out

@@ -167,3 +167,95 @@ def test_slab_configurations_refused():
     with pytest.raises(N.LbmanError) as e:  # outside the box
         SL.Slab(p, L.FullyPeriodicConfig(), L.Precision.FP64, N.KERNELS_SPLIT, 6, 4)
     assert e.value.status == N.ERR_ARG
+
+
+class _LoopbackDist:
+    """torch.distributed stand-in for ranks living in one process: each
+    rank's batch of point-to-point operations is recorded, and flush() pairs
+    the i-th send from rank a to rank b with the i-th receive that b posted
+    from a (NCCL's matching rule) and copies on the device."""
+
+    class P2POp:
+        def __init__(self, op, tensor, peer, group=None):
+            self.op, self.tensor, self.peer = op, tensor, peer
+
+    def __init__(self):
+        self.rank, self.posted = None, {}
+
+    def isend(self, *a):  # identity markers, as in torch.distributed
+        raise AssertionError("called through batch_isend_irecv only")
+
+    def irecv(self, *a):
+        raise AssertionError("called through batch_isend_irecv only")
+
+    def batch_isend_irecv(self, ops):
+        self.posted[self.rank] = list(ops)
+        return []
+
+    def flush(self):
+        sends, recvs = {}, {}
+        for r, ops in self.posted.items():
+            for op in ops:
+                if op.op == self.isend:
+                    sends.setdefault((r, op.peer), []).append(op.tensor)
+                else:
+                    recvs.setdefault((op.peer, r), []).append(op.tensor)
+        assert sends.keys() == recvs.keys()
+        for key, ts in sends.items():
+            assert len(ts) == len(recvs[key])
+            for s, d in zip(ts, recvs[key]):
+                assert s.numel() == d.numel()
+                d.copy_(s)
+        self.posted = {}
+
+
+@pytest.mark.parametrize("planes", [[(0, 5), (5, 7)], [(0, 4), (4, 4), (8, 4)]], ids=["2_ranks", "3_ranks"])
+def test_rank_transport_on_device_memory_equals_the_whole_box(planes):
+    """p2p_exchange with device tensors over the spans' addresses (the
+    DistributedSlab path, ranks emulated in one process): bitwise the box."""
+    import torch
+    from cases import BC
+    grid = (16, 12, 12)
+    p = _params(grid, False, ALPHA=0.02)
+    faces = L.from_face_tuples(BC["channel"])
+    rho, u, q = _state(grid, 3)
+    box = L.Simulation(p, faces, L.Precision.FP64, N.KERNELS_SPLIT)
+    box.upload(rho, u, q)
+    dev = torch.cuda.current_device()
+    cur = torch.cuda.current_stream().cuda_stream
+    slabs = [SL.Slab(p, faces, L.Precision.FP64, N.KERNELS_SPLIT, z0, n, dev) for z0, n in planes]
+    world = len(slabs)
+    nxy = grid[0] * grid[1]
+    parts = [SL._split_field(a, nc, nxy, planes) for a, nc in ((rho, 1), (u, 3), (q, 5))]
+    for s, r, uu, qq in zip(slabs, *parts):
+        s.set_stream(cur)  # the exchange's copies run on torch's current stream
+        s.upload(r, uu, qq)
+
+    def exchange(phase):
+        fake = _LoopbackDist()
+        for r, s in enumerate(slabs):
+            send, recv, nb = s.halo_spans(phase)
+            fake.rank = r
+            SL.p2p_exchange(send, recv, lambda a, nb=nb: SL.device_span(a, nb, dev), r, world, fake)
+        fake.flush()
+        for s in slabs:
+            s.halo_done(phase)
+
+    for _ in range(5):
+        exchange(N.HALO_QU)
+        for s in slabs:
+            s.qtensor_step()
+        exchange(N.HALO_F_IN)
+        for s in slabs:
+            s.lbm_step()
+        exchange(N.HALO_F_OUT)
+    box.step(5)
+    exchange(N.HALO_F_IN)
+    outs = [s.download(f=True) for s in slabs]
+    ref = box.download(f=True)
+    for key, nc in (("rho", 1), ("u", 3), ("q", 5), ("f", 15)):
+        got = np.concatenate([o[key].reshape(nc, -1, nxy) for o in outs], axis=1).reshape(-1)
+        np.testing.assert_array_equal(got, ref[key], err_msg=key)
+    for s in slabs:
+        s.close()
+    box.close()
