@@ -320,6 +320,10 @@ int lbman_ensemble_set_stream(lbman_ensemble* e, void* cuda_stream);
 /* Box b gets lbman_init_seeded's state with seed + b and S0 = its own
  * equilibrium order (src/model.h:39-41).                                    */
 int lbman_ensemble_init_seeded(lbman_ensemble* e, uint64_t seed, double sigma);
+/* The same with one seed per box (box b's field is a single box's
+ * lbman_init_seeded(seeds[b]) field): a rank holding a share of a larger
+ * ensemble seeds its boxes by their index in the whole ensemble.           */
+int lbman_ensemble_init_seeded_each(lbman_ensemble* e, const uint64_t* seeds, double sigma);
 /* Before the first step only: rho, u, Q of one box; f = f_eq, F = 0.       */
 int lbman_ensemble_upload(lbman_ensemble* e, int box, const double* rho, const double* u3, const double* q5);
 int lbman_ensemble_download(lbman_ensemble* e, int box, double* rho, double* u3, double* q5, double* f15);

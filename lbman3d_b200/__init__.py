@@ -11,7 +11,7 @@ from .boundary import (Anchoring, BCConfig, ChannelConfig, FullyPeriodicConfig, 
 from .device import (DeviceFields, DeviceSolver, InitializeComputeBackend, LbmSolver, QTensorSolver,
                      Simulation, make_config)
 from .fields import FluidFields, LocalGrid, QTensorFields
-from .ensemble import Ensemble, draw_boxes
+from .ensemble import Ensemble, ShardedEnsemble, draw_boxes, shard_boxes
 from .params import Advection, EquilibriumScalarOrder, Params, Precision
 from .slab import DistributedSlab, Slab, SlabBox, split_planes
 
@@ -21,5 +21,5 @@ __all__ = [
     "from_face_tuples", "is_wall_by_face", "periodicity_by_axis", "DeviceFields", "DeviceSolver",
     "InitializeComputeBackend", "LbmSolver", "QTensorSolver", "Simulation", "make_config", "FluidFields",
     "LocalGrid", "QTensorFields", "Advection", "EquilibriumScalarOrder", "Params", "Precision", "Ensemble",
-    "draw_boxes", "DistributedSlab", "Slab", "SlabBox", "split_planes",
+    "draw_boxes", "ShardedEnsemble", "shard_boxes", "DistributedSlab", "Slab", "SlabBox", "split_planes",
 ]

@@ -114,6 +114,7 @@ PROTOTYPES = [
     ("lbman_ensemble_destroy", C.c_int, [C.c_void_p]),
     ("lbman_ensemble_set_stream", C.c_int, [C.c_void_p, C.c_void_p]),
     ("lbman_ensemble_init_seeded", C.c_int, [C.c_void_p, C.c_uint64, C.c_double]),
+    ("lbman_ensemble_init_seeded_each", C.c_int, [C.c_void_p, C.POINTER(C.c_uint64), C.c_double]),
     ("lbman_ensemble_upload", C.c_int, [C.c_void_p, C.c_int, _DP, _DP, _DP]),
     ("lbman_ensemble_download", C.c_int, [C.c_void_p, C.c_int, _DP, _DP, _DP, _DP]),
     ("lbman_ensemble_step", C.c_int, [C.c_void_p, C.c_int]),

@@ -289,6 +289,13 @@ int lbman_ensemble_set_stream(lbman_ensemble* e, void* stream) {
 
 int lbman_ensemble_init_seeded(lbman_ensemble* e, uint64_t seed, double sigma) {
     if (!e) return efail(LBMAN_ERR_ARG, "null ensemble");
+    std::vector<uint64_t> seeds((size_t)e->n);
+    for (int b = 0; b < e->n; ++b) seeds[(size_t)b] = seed + (uint64_t)b;
+    return lbman_ensemble_init_seeded_each(e, seeds.data(), sigma);
+}
+
+int lbman_ensemble_init_seeded_each(lbman_ensemble* e, const uint64_t* seeds, double sigma) {
+    if (!e || !seeds) return efail(LBMAN_ERR_ARG, "null argument");
     E_CUDA(cudaSetDevice(e->device));
     e->par = 0;
     for (int b = 0; b < e->n; ++b) {
@@ -296,7 +303,7 @@ int lbman_ensemble_init_seeded(lbman_ensemble* e, uint64_t seed, double sigma) {
         const SimParams& P = B.P;
         // ordered root of the bulk Landau-de Gennes field (src/model.h:39-41)
         const double S0 = (-P.B + std::sqrt(P.B * P.B - 24.0 * P.A * P.C)) / (4.0 * P.C);
-        if (e->ops().seeded_init(P, seed + (uint64_t)b, S0, sigma, B.rho, B.u[0], B.q[0], B.F, e->stream) != cudaSuccess ||
+        if (e->ops().seeded_init(P, seeds[b], S0, sigma, B.rho, B.u[0], B.q[0], B.F, e->stream) != cudaSuccess ||
             e->ops().feq_init(P, B.rho, B.u[0], B.f[0], e->stream) != cudaSuccess)
             return efail(LBMAN_ERR_CUDA, "seeded initialisation failed");
         E_CUDA(cudaMemcpyAsync(B.u[1], B.u[0], 3 * P.V * e->rbytes, cudaMemcpyDeviceToDevice, e->stream));

@@ -44,6 +44,13 @@ class Ensemble:
     def init_seeded(self, seed: int, sigma: float = 1e-3):
         N.check(N.lib().lbman_ensemble_init_seeded(self._h, int(seed), float(sigma)))
 
+    def init_seeded_each(self, seeds, sigma: float = 1e-3):
+        """One seed per box (lbman_ensemble_init_seeded_each)."""
+        s = (C.c_uint64 * len(self.boxes))(*[int(v) for v in seeds])
+        if len(seeds) != len(self.boxes):
+            raise ValueError("one seed per box")
+        N.check(N.lib().lbman_ensemble_init_seeded_each(self._h, s, float(sigma)))
+
     def upload(self, box: int, rho, u, q):
         c = lambda a: np.ascontiguousarray(a, dtype=np.float64)
         N.check(N.lib().lbman_ensemble_upload(self._h, int(box), N.dptr(c(rho)), N.dptr(c(u)), N.dptr(c(q))))
@@ -82,6 +89,43 @@ class Ensemble:
         cells, steps, launches = C.c_int64(), C.c_int64(), C.c_int64()
         N.check(N.lib().lbman_ensemble_info(self._h, C.byref(cells), C.byref(steps), C.byref(launches)))
         return {"cells": cells.value, "steps": steps.value, "launches": launches.value}
+
+
+def shard_boxes(boxes, world: int):
+    """Box indices of each of `world` ranks: a cell-balanced greedy
+    assignment (largest box first, to the least-loaded rank, ties to the
+    lower rank), each rank's list in increasing order.  The loads differ by
+    at most the largest box's cell count."""
+    if world < 1:
+        raise ValueError("world must be >= 1")
+    order = sorted(range(len(boxes)), key=lambda i: (-boxes[i][0].V, i))
+    load, share = [0] * world, [[] for _ in range(world)]
+    for i in order:
+        r = min(range(world), key=lambda k: (load[k], k))
+        load[r] += boxes[i][0].V
+        share[r].append(i)
+    return [sorted(s) for s in share]
+
+
+class ShardedEnsemble(Ensemble):
+    """Rank `rank`'s share of an ensemble spread over `world` GPUs
+    (shard_boxes): the boxes are independent, so the ranks exchange nothing
+    while stepping.  Box ids are indices in the whole ensemble; seeding uses
+    them, so every box's field does not depend on the rank count."""
+
+    def __init__(self, boxes, rank: int, world: int, precision: int = Precision.FP32,
+                 kernels: int = N.KERNELS_AUTO, device: int = 0, tile=None):
+        self.all_boxes = list(boxes)
+        self.ids = shard_boxes(self.all_boxes, world)[rank]
+        self.local = {g: i for i, g in enumerate(self.ids)}
+        super().__init__([self.all_boxes[g] for g in self.ids], precision, kernels, device, tile)
+
+    def init_seeded(self, seed: int, sigma: float = 1e-3):
+        self.init_seeded_each([seed + g for g in self.ids], sigma)
+
+    def download_box(self, box_id: int, f=False):
+        """Fields of box `box_id` (an index in the whole ensemble) held here."""
+        return self.download(self.local[box_id], f=f)
 
 
 SIDES = (24, 32, 48, 64, 96)

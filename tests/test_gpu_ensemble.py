@@ -79,3 +79,24 @@ def test_draw_boxes_matches_the_batching_workload():
         assert p.ny == p.nz and p.nx <= p.ny
         assert 1e-3 <= p.ALPHA <= 3e-2 and 0.1 <= p.LAMBDA <= 0.7
         assert isinstance(bc, L.FullyPeriodicConfig if i % 2 == 0 else L.SlitConfig)
+
+
+@pytest.mark.parametrize("world", [2, 3])
+def test_sharded_ensemble_equals_the_whole_ensemble(world):
+    """The ensemble split over ranks (emulated here as shards in one process
+    on one GPU): every box, seeded by its index in the whole ensemble, ends
+    bitwise where the unsharded ensemble leaves it."""
+    boxes = _boxes()
+    whole = L.Ensemble(boxes, L.Precision.FP32, N.KERNELS_SPLIT, tile=(14, 14, 0))
+    whole.init_seeded(11)
+    whole.step(6)
+    for r in range(world):
+        sh = L.ShardedEnsemble(boxes, r, world, L.Precision.FP32, N.KERNELS_SPLIT, tile=(14, 14, 0))
+        sh.init_seeded(11)
+        sh.step(6)
+        for g in sh.ids:
+            a, b = sh.download_box(g, f=True), whole.download(g, f=True)
+            for k in ("rho", "u", "q", "f"):
+                np.testing.assert_array_equal(a[k], b[k], err_msg=f"box {g} {k}")
+        sh.close()
+    whole.close()

@@ -181,3 +181,19 @@ def test_exchange_between_ranks_fills_exactly_the_planned_ghosts(world, nzg):
             np.testing.assert_array_equal(S[0, i], code(7, k, z0, nzg) + 0.5)
         for i, k in enumerate(DOWN):
             np.testing.assert_array_equal(S[1, i], code(7, k, z0 + nzl - 1, nzg) + 0.5)
+
+
+# ---- the ensemble across ranks (no exchange) --------------------------------
+
+
+@pytest.mark.parametrize("world", [1, 2, 3, 8])
+def test_shard_boxes_is_a_cell_balanced_partition(world):
+    import lbman3d_b200 as L
+    boxes = L.draw_boxes(96, seed=2024)
+    shares = L.shard_boxes(boxes, world)
+    ids = sorted(i for s in shares for i in s)
+    assert ids == list(range(96))
+    assert all(s == sorted(s) for s in shares)
+    loads = [sum(boxes[i][0].V for i in s) for s in shares]
+    assert max(loads) - min(loads) <= max(p.V for p, _ in boxes)
+    assert shares == L.shard_boxes(boxes, world)  # deterministic
