@@ -407,14 +407,26 @@ int lbman_closure_gradient(lbman_closure* c, const float* feat9, const float* ta
  * f times the closure grid on every axis; new_trajectory starts a new
  * sequence (pairs never span two sequences).                              */
 int lbman_closure_record(lbman_closure* c, lbman_solver* fine, int new_trajectory);
+/* The same from box `box` of an ensemble (the training data of many fine
+ * runs advanced together), as a snapshot of trajectory `trajectory` (>= 0,
+ * the caller's id; one id per box).                                        */
+int lbman_closure_record_box(lbman_closure* c, lbman_ensemble* e, int box, int trajectory);
 int lbman_closure_dataset(lbman_closure* c, int* snapshots, int* pairs);
-/* For each consecutive snapshot pair (k, k+1) of a sequence, the target
- * snapshot(k+1) - coarse_step(snapshot k), where coarse_step rebuilds the
+/* For each snapshot k and the next snapshot k' of its trajectory, the target
+ * snapshot(k') - coarse_step(snapshot k), where coarse_step rebuilds the
  * populations as f_eq and takes one step of the coarse solver (FP32/FP16 on
  * the closure grid, with the coarse-grid parameters).  fit_scales sets the
  * input shift/scale to the per-channel mean/std of the snapshots and the
  * output scales to the rms target of Q and of u.                          */
 int lbman_closure_build_targets(lbman_closure* c, lbman_solver* coarse, int fit_scales);
+/* Rollout ("pushforward") pairs: from every stride-th snapshot k that has a
+ * snapshot k'' m + 1 recordings later in its trajectory, m corrected coarse
+ * steps with the current network give the state x the corrected run is in;
+ * the pair is (x, snapshot(k'') - coarse_step(x)).  Training on them teaches
+ * the network to correct its own accumulated error.  Appended to the pairs
+ * of lbman_closure_build_targets (which clears both); *added receives the
+ * count.                                                                   */
+int lbman_closure_add_rollout_pairs(lbman_closure* c, lbman_solver* coarse, int m, int stride, int* added);
 /* Adam (beta 0.9 / 0.999) on random training pairs; loss_first/last receive
  * the mean loss of the first and last tenth of the iterations.            */
 int lbman_closure_train(lbman_closure* c, int iters, float lr, uint64_t seed, double* loss_first, double* loss_last);

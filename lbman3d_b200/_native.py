@@ -143,6 +143,9 @@ PROTOTYPES = [
     ("lbman_closure_forward", C.c_int, [C.c_void_p, _FP, _FP]),
     ("lbman_closure_gradient", C.c_int, [C.c_void_p, _FP, _FP, _DP, _FP]),
     ("lbman_closure_record", C.c_int, [C.c_void_p, C.c_void_p, C.c_int]),
+    ("lbman_closure_record_box", C.c_int, [C.c_void_p, C.c_void_p, C.c_int, C.c_int]),
+    ("lbman_closure_add_rollout_pairs", C.c_int, [C.c_void_p, C.c_void_p, C.c_int, C.c_int,
+                                                  C.POINTER(C.c_int)]),
     ("lbman_closure_dataset", C.c_int, [C.c_void_p, C.POINTER(C.c_int), C.POINTER(C.c_int)]),
     ("lbman_closure_build_targets", C.c_int, [C.c_void_p, C.c_void_p, C.c_int]),
     ("lbman_closure_train", C.c_int, [C.c_void_p, C.c_int, C.c_float, C.c_uint64, _DP, _DP]),

@@ -103,6 +103,16 @@ class Closure:
     def record(self, fine, new_trajectory: bool = False):
         N.check(N.lib().lbman_closure_record(self._h, fine.handle, int(bool(new_trajectory))))
 
+    def record_box(self, ensemble, box: int, trajectory: int):
+        """Snapshot of ensemble box `box` as trajectory `trajectory`."""
+        N.check(N.lib().lbman_closure_record_box(self._h, ensemble._h, int(box), int(trajectory)))
+
+    def add_rollout_pairs(self, coarse, m: int, stride: int = 1) -> int:
+        """Pairs from m-step corrected runs (lbman_closure_add_rollout_pairs)."""
+        n = C.c_int()
+        N.check(N.lib().lbman_closure_add_rollout_pairs(self._h, coarse.handle, int(m), int(stride), C.byref(n)))
+        return n.value
+
     def dataset(self):
         a, b = C.c_int(), C.c_int()
         N.check(N.lib().lbman_closure_dataset(self._h, C.byref(a), C.byref(b)))

@@ -4,10 +4,15 @@ and measure it against a held-out fine run and against the plain coarse solver.
     python -m lbman3d_b200.closure_experiment [--fine 256] [--factor 4] ...
 
 Fine runs: FullyPeriodic, FP32, seeded random director (S0 = equilibrium
-order, 1e-3 Gaussian), zeta = ALPHA.  Every ``factor`` fine steps the fine
-state is box-filtered onto the coarse grid (one coarse step = ``factor``
-fine steps, coarse parameters from closure.coarse_params).  Training pairs
-come from the training seeds; the held-out seed is the yardstick:
+order, 1e-3 Gaussian), zeta = ALPHA.  The training runs advance together in
+one ensemble (one box per training seed); every ``factor`` fine steps each
+box's state is box-filtered onto the coarse grid straight from the device
+(one coarse step = ``factor`` fine steps, coarse parameters from
+closure.coarse_params).  Training is one-step pairs first, then rounds of
+rollout ("pushforward") pairs: the corrected coarse run is advanced m steps
+from a filtered snapshot with the current network, and the pair asks for the
+correction that brings that drifted state back onto the filtered fine run
+(``--push-m``, ``--push-iters``).  The held-out seed is the yardstick:
 
 * short-time error: relative L2 error of coarse Q and u against the
   filtered fine run after n coarse steps from the same filtered start, for
@@ -52,7 +57,8 @@ def _rel(a, b):
 
 
 def run(fine_n=256, factor=4, zeta=0.01, train_seeds=(11, 12, 13), test_seed=99, burn=2000, snaps=120,
-        iters=3000, lr=1e-3, rollout=100, tolerance=0.05, train_noise=0.05, log=print):
+        iters=3000, lr=1e-3, rollout=100, tolerance=0.05, train_noise=0.05, push_m=(), push_iters=2000,
+        push_stride=2, log=print):
     import torch
 
     import lbman3d_b200 as L
@@ -65,11 +71,12 @@ def run(fine_n=256, factor=4, zeta=0.01, train_seeds=(11, 12, 13), test_seed=99,
     bc = L.FullyPeriodicConfig()
     nc = fine_n // factor
     nbins = nc // 2
-    stream = torch.cuda.current_stream()
+    stream = torch.cuda.Stream()  # a capturable stream: the ensemble replays its steps from CUDA graphs
     res = {"fine_grid": [fine_n] * 3, "coarse_grid": [nc] * 3, "factor": factor, "zeta": zeta,
            "train_seeds": list(train_seeds), "test_seed": test_seed, "burn_in_steps": burn,
            "snapshots_per_seed": snaps, "train_iters": iters, "lr": lr, "train_input_noise": train_noise,
-           "rollout_coarse_steps": rollout,
+           "rollout_coarse_steps": rollout, "push_m": list(push_m), "push_iters": push_iters,
+           "push_stride": push_stride,
            "coarse_params": {"TAUF": cp.TAUF, "GAMMA": cp.GAMMA, "L": cp.L, "ALPHA": cp.ALPHA}}
 
     fine = L.Simulation(fp, bc, L.Precision.FP32)
@@ -81,27 +88,43 @@ def run(fine_n=256, factor=4, zeta=0.01, train_seeds=(11, 12, 13), test_seed=99,
     cl = CL.Closure(nc, nc, nc, seed=1)
     cl.set_options(train_noise=train_noise)
 
-    # --- training data ---------------------------------------------------------
-    for sd in train_seeds:
-        fine.init_seeded(sd, S0, 1e-3)
-        fine.step(burn)
-        cl.record(fine, new_trajectory=True)
-        for _ in range(snaps):
-            fine.step(factor)
-            cl.record(fine)
+    # --- training data: the training runs advance together in one ensemble ------
+    ens = L.Ensemble([(fp, bc)] * len(train_seeds), L.Precision.FP32, device=torch.cuda.current_device())
+    ens.set_stream(stream.cuda_stream)
+    ens.init_seeded_each(list(train_seeds), 1e-3)
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record(stream)
+    ens.step(burn)
+    for b in range(len(train_seeds)):
+        cl.record_box(ens, b, b)
+    for _ in range(snaps):
+        ens.step(factor)
+        for b in range(len(train_seeds)):
+            cl.record_box(ens, b, b)
+    e1.record(stream)
+    e1.synchronize()
+    res["ensemble"] = {"boxes": len(train_seeds), "cells": len(train_seeds) * fp.V,
+                       "fine_steps": burn + snaps * factor, "ms": e0.elapsed_time(e1),
+                       "mlups": len(train_seeds) * fp.V * (burn + snaps * factor) / (e0.elapsed_time(e1) * 1e3)}
+    ens.close()
     cl.build_targets(coarse)
     res["dataset"] = dict(zip(("snapshots", "pairs"), cl.dataset()))
     log(f"data ready: {res['dataset']} ({time.time() - t0:.1f} s)")
 
-    # --- training ----------------------------------------------------------------
-    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    # --- training: one-step pairs, then rounds of rollout pairs ------------------
     e0.record(stream)
     first, last = cl.train(iters, lr=lr, seed=7)
     e1.record(stream)
     e1.synchronize()
     res["train"] = {"loss_first_tenth": first, "loss_last_tenth": last,
-                    "ms_per_iteration": e0.elapsed_time(e1) / iters}
+                    "ms_per_iteration": e0.elapsed_time(e1) / iters, "rounds": []}
     log(f"trained: loss {first:.4g} -> {last:.4g} ({time.time() - t0:.1f} s)")
+    for r, m in enumerate(push_m):
+        added = cl.add_rollout_pairs(coarse, int(m), push_stride)
+        first, last = cl.train(push_iters, lr=lr * 0.5, seed=100 + r)
+        res["train"]["rounds"].append({"m": int(m), "pairs_added": added, "pairs": cl.dataset()[1],
+                                       "loss_first_tenth": first, "loss_last_tenth": last})
+        log(f"rollout round m={m}: +{added} pairs, loss {first:.4g} -> {last:.4g} ({time.time() - t0:.1f} s)")
 
     # --- held-out run: filtered fine trajectory --------------------------------
     n0, _ = cl.dataset()
@@ -202,10 +225,15 @@ def main(argv=None):
     ap.add_argument("--tolerance", type=float, default=0.05)
     ap.add_argument("--train-noise", type=float, default=0.05,
                     help="std of Gaussian noise on the normalised inputs while training")
+    ap.add_argument("--push-m", default="", help="comma-separated rollout lengths of the pushforward rounds")
+    ap.add_argument("--push-iters", type=int, default=2000)
+    ap.add_argument("--push-stride", type=int, default=2)
     a = ap.parse_args(argv)
     import sys
+    push = tuple(int(v) for v in a.push_m.split(",") if v.strip())
     res = run(a.fine, a.factor, a.zeta, tuple(range(11, 11 + a.seeds)), 99, a.burn, a.snaps, a.iters, a.lr,
-              a.rollout, a.tolerance, a.train_noise, log=lambda m: print(m, file=sys.stderr, flush=True))
+              a.rollout, a.tolerance, a.train_noise, push, a.push_iters, a.push_stride,
+              log=lambda m: print(m, file=sys.stderr, flush=True))
     print(json.dumps(res))
 
 

@@ -243,117 +243,143 @@ __global__ void __launch_bounds__(kThreads) conv_kernel(Grid3 g, const __nv_bflo
     if (t < 32) tc::tmem_dealloc(tmem, 32);
 }
 
-// ---- descriptor-halo convolution -------------------------------------------
+// ---- descriptor-halo convolution, z-marching ---------------------------------
 // Tile = 8 x-cells by 16 y-rows of one z plane (128 cells, M row m = 8*dy_row
-// + dx_cell).  The tile's neighbourhood (10 x 18 x 3 cells) is staged once
-// as 16-byte units, one plane per 8-channel group:
-//   unit(kg, hz, hy, hx) at ((kg*3 + hz)*18 + hy)*10 + hx,
-// which makes the A operand of every tap a K-major view of the halo: rows
-// of a core matrix are 8 consecutive x cells (16 bytes apart), the next
-// y row is SBO = 160 bytes on, the next 8 channels LBO = 8640 bytes on, and
-// the tap shift (dx, dy, dz) only moves the start address.  So each tile is
-// one halo copy and 27 x CIN/16 back-to-back MMAs with no operand copies;
-// the halo and the TMEM accumulator are double-buffered so the next tile's
-// copy and this tile's epilogue overlap the tensor core.
-constexpr int kHX = 10, kHY = 18, kHZ = 3;
-constexpr int kHaloPlane = kHX * kHY * kHZ * 16;  // bytes per 8-channel group
+// + dx_cell).  A CTA takes a column of tiles (the same 8 x 16 block of every
+// plane of a z range) and marches it in z.  The column's neighbourhood is
+// staged plane by plane (10 x 18 cells per plane) in a ring of 5 plane slots,
+// as 16-byte units, one block per 8-channel group:
+//   unit(slot, kg, hy, hx) at slot*SLOT + (kg*18 + hy)*10 + hx,
+// which makes the A operand of every tap a K-major view of the ring: rows of
+// a core matrix are 8 consecutive x cells (16 bytes apart), the next y row is
+// SBO = 160 bytes on, the next 8 channels LBO = 2880 bytes on, and the tap
+// (dx, dy, dz) only picks the slot of plane z + dz and moves the start
+// address.  So each tile costs one new plane (the other two are the previous
+// tiles') and 27 x CIN/16 back-to-back MMAs with no operand copies; the copy
+// of a plane is issued two tiles before the tile that first reads it.  The
+// TMEM accumulator is double buffered.  Warps 0-7 copy planes and run the
+// epilogues (warps w and w + 4 read the same TMEM lanes, 32 (w % 4) ..,
+// and split the accumulator's columns); warp 8 issues the MMAs.  So while
+// the tensor core runs tile z, warps 0-7 start copying plane z + 3, finish
+// tile z - 1 and wait for plane z + 2, and warp 8 has queued tile z: one
+// block barrier per tile.
+constexpr int kHX = 10, kHY = 18;
+constexpr int kZWorkers = 256;             // copy / epilogue threads
+constexpr int kZThreads = kZWorkers + 32;  // + the MMA warp
+constexpr int kZIssuer = kZWorkers;        // the thread that issues the MMAs
+constexpr int kSlots = 5;
+__host__ __device__ constexpr int ring_slot(int plane) { return (plane + kSlots) % kSlots; }  // plane >= -1
+__host__ __device__ constexpr int dhalo_slot_bytes(int cin) { return (cin / 8) * kHX * kHY * 16; }
+__host__ __device__ constexpr int dhalo_bytes(int cin) { return kSlots * dhalo_slot_bytes(cin); }
 
 __host__ __device__ inline bool dhalo_ok(int nx, int ny) { return nx % 8 == 0 && ny % 16 == 0; }
-__host__ __device__ constexpr int dhalo_bytes(int cin) { return (cin / 8) * kHaloPlane; }
 
+// Copies plane zz (-1 <= zz <= nz, periodic) of the column at (x0, y0) into
+// its ring slot S (worker threads).
 template <int CIN>
-__device__ __forceinline__ void dhalo_load(const Grid3& g, const __nv_bfloat16* __restrict__ in, int x0, int y0,
-                                           int z0, unsigned char* H) {
-    constexpr int QU = CIN / 8;
-    constexpr int N = QU * kHX * kHY * kHZ;
-    for (int i = threadIdx.x; i < N; i += kThreads) {
-        const int hx = i % kHX, hy = (i / kHX) % kHY, hz = (i / (kHX * kHY)) % kHZ, kg = i / (kHX * kHY * kHZ);
-        const int64_t cell =
-            ((int64_t)wrapi(z0 - 1 + hz, g.nz) * g.ny + wrapi(y0 - 1 + hy, g.ny)) * g.nx + wrapi(x0 - 1 + hx, g.nx);
+__device__ __forceinline__ void dhalo_load_plane(const Grid3& g, const __nv_bfloat16* __restrict__ in, int x0,
+                                                 int y0, int zz, unsigned char* S) {
+    constexpr int N = (CIN / 8) * kHX * kHY;
+    const int64_t zoff = (int64_t)wrapi(zz, g.nz) * g.ny;
+    for (int i = threadIdx.x; i < N; i += kZWorkers) {
+        const int hx = i % kHX, hy = (i / kHX) % kHY, kg = i / (kHX * kHY);
+        const int64_t cell = (zoff + wrapi(y0 - 1 + hy, g.ny)) * g.nx + wrapi(x0 - 1 + hx, g.nx);
         const uint4* src = reinterpret_cast<const uint4*>(in + cell * CIN) + kg;
-        asm volatile("cp.async.cg.shared.global [%0], [%1], 16;\n" ::"r"(tc::smem_addr(H + i * 16)), "l"(src));
+        asm volatile("cp.async.cg.shared.global [%0], [%1], 16;\n" ::"r"(tc::smem_addr(S + i * 16)), "l"(src));
     }
 }
 
+// Epilogue of one tile: this thread's cell c (TMEM lane = threadIdx % 128)
+// and its half of the COUT accumulator columns (bias: that half's biases).
 template <int COUT, int MODE>
-__device__ __forceinline__ void conv_epilogue(uint32_t tacc, int64_t c, const float* __restrict__ bias,
+__device__ __forceinline__ void conv_epilogue(uint32_t tacc, int64_t c, const float (&bias)[COUT / 2],
                                               const __nv_bfloat16* __restrict__ pre_below,
                                               __nv_bfloat16* __restrict__ out_pre, __nv_bfloat16* __restrict__ out_bf,
                                               float* __restrict__ out_f) {
-    const int w = threadIdx.x >> 5;
-    float acc[COUT];
-#pragma unroll
-    for (int c0 = 0; c0 < COUT; c0 += 16) tc::tmem_ld16(tacc + ((uint32_t)(32 * w) << 16) + (uint32_t)c0, acc + c0);
+    constexpr int H = COUT / 2;
+    static_assert(H == 8 || H == 16, "16 or 32 output channels");
+    const int w = threadIdx.x >> 5, half = threadIdx.x >> 7;
+    const int j0 = half * H;
+    float acc[H];
+    const uint32_t ta = tacc + ((uint32_t)(32 * (w & 3)) << 16) + (uint32_t)j0;
+    if constexpr (H == 16) tc::tmem_ld16(ta, acc);
+    else tc::tmem_ld8(ta, acc);
     if constexpr (MODE == kFwdHidden) {
-        __align__(16) __nv_bfloat16 pb[COUT], ab[COUT];
+        __align__(16) __nv_bfloat16 pb[H], ab[H];
 #pragma unroll
-        for (int j = 0; j < COUT; ++j) {
+        for (int j = 0; j < H; ++j) {
             const float p = acc[j] + bias[j];
             pb[j] = __float2bfloat16(p);
             ab[j] = __float2bfloat16(gelu(p));
         }
 #pragma unroll
-        for (int q = 0; q < COUT / 8; ++q) {
-            reinterpret_cast<uint4*>(out_pre + c * COUT)[q] = reinterpret_cast<const uint4*>(pb)[q];
-            reinterpret_cast<uint4*>(out_bf + c * COUT)[q] = reinterpret_cast<const uint4*>(ab)[q];
+        for (int q = 0; q < H / 8; ++q) {
+            reinterpret_cast<uint4*>(out_pre + c * COUT + j0)[q] = reinterpret_cast<const uint4*>(pb)[q];
+            reinterpret_cast<uint4*>(out_bf + c * COUT + j0)[q] = reinterpret_cast<const uint4*>(ab)[q];
         }
     } else if constexpr (MODE == kFwdLast) {
 #pragma unroll
-        for (int j = 0; j < COUT; j += 4)
-            reinterpret_cast<float4*>(out_f + c * COUT)[j / 4] = make_float4(
-                acc[j] + bias[j], acc[j + 1] + bias[j + 1], acc[j + 2] + bias[j + 2], acc[j + 3] + bias[j + 3]);
+        for (int j = 0; j < H; j += 4)
+            reinterpret_cast<float4*>(out_f + c * COUT + j0)[j / 4] =
+                make_float4(acc[j] + bias[j], acc[j + 1] + bias[j + 1], acc[j + 2] + bias[j + 2],
+                            acc[j + 3] + bias[j + 3]);
     } else {
-        __align__(16) __nv_bfloat16 pre[COUT], gb[COUT];
+        __align__(16) __nv_bfloat16 pre[H], gb[H];
 #pragma unroll
-        for (int q = 0; q < COUT / 8; ++q)
-            reinterpret_cast<uint4*>(pre)[q] = reinterpret_cast<const uint4*>(pre_below + c * COUT)[q];
+        for (int q = 0; q < H / 8; ++q)
+            reinterpret_cast<uint4*>(pre)[q] = reinterpret_cast<const uint4*>(pre_below + c * COUT + j0)[q];
 #pragma unroll
-        for (int j = 0; j < COUT; ++j) gb[j] = __float2bfloat16(acc[j] * gelu_grad(__bfloat162float(pre[j])));
+        for (int j = 0; j < H; ++j) gb[j] = __float2bfloat16(acc[j] * gelu_grad(__bfloat162float(pre[j])));
 #pragma unroll
-        for (int q = 0; q < COUT / 8; ++q)
-            reinterpret_cast<uint4*>(out_bf + c * COUT)[q] = reinterpret_cast<const uint4*>(gb)[q];
+        for (int q = 0; q < H / 8; ++q)
+            reinterpret_cast<uint4*>(out_bf + c * COUT + j0)[q] = reinterpret_cast<const uint4*>(gb)[q];
     }
 }
 
-// Smem: B image, then two halo buffers.  TMEM: two 32-column accumulators.
+// Block b marches column b % cols over planes [zc * (b / cols), + zc).
+// Smem: B image, then the plane ring.  TMEM: two 32-column accumulators.
 template <int CIN, int COUT, int MODE>
-__global__ void __launch_bounds__(kThreads) conv_dhalo_kernel(Grid3 g, const __nv_bfloat16* __restrict__ in,
-                                                              const uint4* __restrict__ bimg,
-                                                              const float* __restrict__ bias,
-                                                              const __nv_bfloat16* __restrict__ pre_below,
-                                                              __nv_bfloat16* __restrict__ out_pre,
-                                                              __nv_bfloat16* __restrict__ out_bf,
-                                                              float* __restrict__ out_f, int* __restrict__ err,
-        uint32_t wait_limit) {
+__global__ void __launch_bounds__(kZThreads) conv_dhalo_kernel(Grid3 g, int zc, const __nv_bfloat16* __restrict__ in,
+                                                               const uint4* __restrict__ bimg,
+                                                               const float* __restrict__ bias,
+                                                               const __nv_bfloat16* __restrict__ pre_below,
+                                                               __nv_bfloat16* __restrict__ out_pre,
+                                                               __nv_bfloat16* __restrict__ out_bf,
+                                                               float* __restrict__ out_f, int* __restrict__ err,
+                                                               uint32_t wait_limit) {
     constexpr int KS = CIN / 16;
     constexpr int BBYTES = bimg_bytes(CIN, COUT);
-    constexpr int HB = dhalo_bytes(CIN);
+    constexpr int SLOT = dhalo_slot_bytes(CIN);
+    constexpr uint32_t KG = kHX * kHY;  // 16-byte units between 8-channel groups
     extern __shared__ __align__(1024) unsigned char sm[];
     __shared__ uint64_t bar[2];
     __shared__ uint32_t tslot;
     unsigned char* Bs = sm;
     unsigned char* Hs = sm + BBYTES;
     const int t = threadIdx.x;
-    for (int i = t; i < BBYTES / 16; i += kThreads) reinterpret_cast<uint4*>(Bs)[i] = bimg[i];
+    for (int i = t; i < BBYTES / 16; i += kZThreads) reinterpret_cast<uint4*>(Bs)[i] = bimg[i];
     if (t == 0) {
         tc::mbar_init(&bar[0], 1);
         tc::mbar_init(&bar[1], 1);
         tc::mbar_fence_init();
     }
     if (t < 32) tc::tmem_alloc(&tslot, 64);
-    const int bx = g.nx / 8, by = g.ny / 16;
-    const int64_t ntiles = (int64_t)bx * by * g.nz;
-    auto origin = [&](int64_t tile, int& x0, int& y0, int& z0) {
-        x0 = (int)(tile % bx) * 8;
-        y0 = (int)((tile / bx) % by) * 16;
-        z0 = (int)(tile / ((int64_t)bx * by));
-    };
-    int x0, y0, z0;
-    if (blockIdx.x < ntiles) {
-        origin(blockIdx.x, x0, y0, z0);
-        dhalo_load<CIN>(g, in, x0, y0, z0, Hs);
+    const int bx = g.nx / 8, cols = bx * (g.ny / 16);
+    const int col = (int)(blockIdx.x % (unsigned)cols);
+    const int x0 = (col % bx) * 8, y0 = (col / bx) * 16;
+    const int za = (int)(blockIdx.x / (unsigned)cols) * zc, zb = min(za + zc, g.nz);
+    const bool worker = t < kZWorkers;
+    float bias_h[COUT / 2];  // this worker's half of the biases
+#pragma unroll
+    for (int j = 0; j < COUT / 2; ++j) bias_h[j] = worker ? bias[((t >> 7) & 1) * (COUT / 2) + j] : 0.0f;
+    if (worker) {
+        for (int zz = za - 1; zz <= za + 1 && za < zb; ++zz)
+            dhalo_load_plane<CIN>(g, in, x0, y0, zz, Hs + ring_slot(zz) * SLOT);
+        asm volatile("cp.async.commit_group;\n" ::: "memory");
+        if (za + 2 <= zb) dhalo_load_plane<CIN>(g, in, x0, y0, za + 2, Hs + ring_slot(za + 2) * SLOT);
+        asm volatile("cp.async.commit_group;\n" ::: "memory");
     }
-    asm volatile("cp.async.wait_all;\n" ::: "memory");
+    asm volatile("cp.async.wait_group 1;\n" ::: "memory");  // planes za-1 .. za+1 in; za+2 may be in flight
     tc::fence_smem_async();
     tc::fence_before_sync();
     __syncthreads();
@@ -361,68 +387,69 @@ __global__ void __launch_bounds__(kThreads) conv_dhalo_kernel(Grid3 g, const __n
     const uint32_t tmem = tslot;
     const uint32_t idesc = tc::idesc_bf16(kTileM, COUT, 0, 0);
     const uint32_t h0 = tc::smem_addr(Hs), b0 = tc::smem_addr(Bs);
+    // a worker's cell in a tile of plane z: M row t % 128
+    const int64_t cxy = (int64_t)(y0 + (t & 127) / 8) * g.nx + x0 + (t & 7);
     uint32_t uses[2] = {0, 0};
     bool ok = true;
-    int64_t prev = -1;  // tile whose epilogue is pending
     int n = 0;
-    for (int64_t tile = blockIdx.x; tile < ntiles && ok; tile += gridDim.x, ++n) {
+    for (int z = za; z < zb && ok; ++z, ++n) {
         const int b = n & 1;
-        if (t == 0) {
-            // the start address is the descriptor's low field (16-byte units,
-            // smem < 256 KB so no carry): tap offsets are added to it directly
-            const uint64_t da0 = tc::smem_desc(h0 + b * HB, kHaloPlane, kHX * 16);
+        if (t == kZIssuer) {
+            // planes z-1 .. z+1 were copied before the last barrier, and the
+            // previous tile of accumulator b (z - 2) was read before it
             const uint64_t db0 = tc::smem_desc(b0, 128, 256);
 #pragma unroll
             for (int tap = 0; tap < 27; ++tap) {
                 const int dx = tap % 3 - 1, dy = (tap / 3) % 3 - 1, dz = tap / 9 - 1;
+                // the start address is the descriptor's low field (16-byte
+                // units, smem < 256 KB so no carry): offsets add directly
+                const uint64_t da = tc::smem_desc(h0 + ring_slot(z + dz) * SLOT, KG * 16, kHX * 16);
 #pragma unroll
                 for (int kb = 0; kb < KS; ++kb) {
-                    const uint32_t aoff = (uint32_t)((((2 * kb) * kHZ + 1 + dz) * kHY + 1 + dy) * kHX + 1 + dx);
+                    const uint32_t aoff = 2 * kb * KG + (uint32_t)((1 + dy) * kHX + 1 + dx);
                     const uint32_t boff = (uint32_t)((tap * KS + kb) * COUT * 32 / 16);
-                    tc::mma_bf16(tmem + b * 32, da0 + aoff, db0 + boff, idesc, (tap > 0 || kb > 0) ? 1u : 0u);
+                    tc::mma_bf16(tmem + b * 32, da + aoff, db0 + boff, idesc, (tap > 0 || kb > 0) ? 1u : 0u);
                 }
             }
             tc::mma_commit(&bar[b]);
         }
         ++uses[b];
-        // stage the next tile's halo in the other buffer once the MMAs that
-        // read it (tile n-1) are done -- that wait also covers the pending epilogue
-        const int64_t next = tile + gridDim.x;
-        bool lost = uses[b ^ 1] > 0 && !tc::mbar_wait(&bar[b ^ 1], (uses[b ^ 1] - 1) & 1, err, wait_limit);
-        if (__syncthreads_or(lost)) {
+        bool lost = false;
+        if (worker) {
+            // tile z - 1 done: its accumulator is final, and the slot of plane
+            // z - 2, which only it still read, takes plane z + 3
+            if (uses[b ^ 1] > 0) lost = !tc::mbar_wait(&bar[b ^ 1], (uses[b ^ 1] - 1) & 1, err, wait_limit);
+            if (!lost) {
+                tc::fence_after_sync();
+                if (z + 3 <= zb) dhalo_load_plane<CIN>(g, in, x0, y0, z + 3, Hs + ring_slot(z + 3) * SLOT);
+                asm volatile("cp.async.commit_group;\n" ::: "memory");
+                if (z > za)
+                    conv_epilogue<COUT, MODE>(tmem + (b ^ 1) * 32, (int64_t)(z - 1) * g.nx * g.ny + cxy, bias_h,
+                                              pre_below, out_pre, out_bf, out_f);
+            }
+            // plane z + 2 in (tile z + 1 reads it); z + 3 may stay in flight
+            if (lost) asm volatile("cp.async.wait_all;\n" ::: "memory");
+            else asm volatile("cp.async.wait_group 1;\n" ::: "memory");
+            tc::fence_smem_async();
+        }
+        tc::fence_before_sync();
+        if (__syncthreads_or(lost)) {  // plane z + 2 visible; accumulator b^1 read
             ok = false;
             break;
         }
         tc::fence_after_sync();
-        if (next < ntiles) {
-            int nx0, ny0, nz0;
-            origin(next, nx0, ny0, nz0);
-            dhalo_load<CIN>(g, in, nx0, ny0, nz0, Hs + (b ^ 1) * HB);
-        }
-        if (prev >= 0) {
-            int px, py, pz;
-            origin(prev, px, py, pz);
-            const int64_t c = ((int64_t)pz * g.ny + py + t / 8) * g.nx + px + t % 8;
-            conv_epilogue<COUT, MODE>(tmem + (b ^ 1) * 32, c, bias, pre_below, out_pre, out_bf, out_f);
-        }
-        asm volatile("cp.async.wait_all;\n" ::: "memory");
-        tc::fence_smem_async();
-        tc::fence_before_sync();
-        __syncthreads();  // next halo visible; accumulator b^1 read before its next MMAs
-        tc::fence_after_sync();
-        prev = tile;
     }
-    if (ok && prev >= 0) {
+    if (ok && n > 0) {
         const int b = (n - 1) & 1;
-        const bool lost = !tc::mbar_wait(&bar[b], (uses[b] - 1) & 1, err, wait_limit);
-        if (!__syncthreads_or(lost)) {
+        bool lost = false;
+        if (worker) lost = !tc::mbar_wait(&bar[b], (uses[b] - 1) & 1, err, wait_limit);
+        if (!__syncthreads_or(lost) && worker) {
             tc::fence_after_sync();
-            int px, py, pz;
-            origin(prev, px, py, pz);
-            const int64_t c = ((int64_t)pz * g.ny + py + t / 8) * g.nx + px + t % 8;
-            conv_epilogue<COUT, MODE>(tmem + b * 32, c, bias, pre_below, out_pre, out_bf, out_f);
+            conv_epilogue<COUT, MODE>(tmem + b * 32, (int64_t)(zb - 1) * g.nx * g.ny + cxy, bias_h, pre_below,
+                                      out_pre, out_bf, out_f);
         }
     }
+    asm volatile("cp.async.wait_all;\n" ::: "memory");  // no copy outlives the block
     if (t == 0) {
         for (int s = 0; s < 2; ++s)
             if (uses[s] > 0) tc::mbar_wait(&bar[s], (uses[s] - 1) & 1, err);
@@ -571,8 +598,28 @@ __global__ void __launch_bounds__(kThreads) wgrad_kernel(Grid3 g, const __nv_bfl
     if (t < 32) tc::tmem_dealloc(tmem, WS::TCOLS);
 }
 
+// The weight gradient's per-tile halo: the 10 x 18 x 3 neighbourhood of an
+// 8 x 16 x 1 tile as 16-byte units, one block per 8-channel group:
+//   unit(kg, hz, hy, hx) at ((kg*3 + hz)*18 + hy)*10 + hx.
+constexpr int kHZ = 3;
+__host__ __device__ constexpr int whalo_bytes(int cin) { return (cin / 8) * kHX * kHY * kHZ * 16; }
+
+template <int CIN>
+__device__ __forceinline__ void whalo_load(const Grid3& g, const __nv_bfloat16* __restrict__ in, int x0, int y0,
+                                           int z0, unsigned char* H) {
+    constexpr int QU = CIN / 8;
+    constexpr int N = QU * kHX * kHY * kHZ;
+    for (int i = threadIdx.x; i < N; i += kThreads) {
+        const int hx = i % kHX, hy = (i / kHX) % kHY, hz = (i / (kHX * kHY)) % kHZ, kg = i / (kHX * kHY * kHZ);
+        const int64_t cell =
+            ((int64_t)wrapi(z0 - 1 + hz, g.nz) * g.ny + wrapi(y0 - 1 + hy, g.ny)) * g.nx + wrapi(x0 - 1 + hx, g.nx);
+        const uint4* src = reinterpret_cast<const uint4*>(in + cell * CIN) + kg;
+        asm volatile("cp.async.cg.shared.global [%0], [%1], 16;\n" ::"r"(tc::smem_addr(H + i * 16)), "l"(src));
+    }
+}
+
 // Weight gradient on 8 x 16 x 1 tiles (nx % 8 == 0, ny % 16 == 0).  Per tile
-// the activation halo (same layout as conv_dhalo_kernel) and the tile's
+// the activation halo (above) and the tile's
 // output gradient are staged once; then for each group of TPG taps the
 // MN-major A operand (rows (tap, ci), K = the tile's 128 cells) is assembled
 // from the halo by 16-byte copies -- cell k of the tile is row k of every
@@ -584,7 +631,7 @@ struct WGradHalo {
     static constexpr int TPG = kTileM / CIN;
     static constexpr int G = (27 + TPG - 1) / TPG;
     static constexpr int TCOLS = WGradShape<CIN, COUT>::TCOLS;
-    static constexpr int HB = dhalo_bytes(CIN);
+    static constexpr int HB = whalo_bytes(CIN);
     static constexpr int BB = (COUT / 8) * 2048;  // output-gradient tile
     static constexpr int AB = 16 * 2048;          // one A buffer (128 x 128 BF16)
     static constexpr int SMEM = HB + BB + 2 * AB;
@@ -631,7 +678,7 @@ __global__ void __launch_bounds__(kThreads) wgrad_dhalo_kernel(Grid3 g, const __
             ok = false;
             break;
         }
-        dhalo_load<CIN>(g, act, x0, y0, z0, Hs);
+        whalo_load<CIN>(g, act, x0, y0, z0, Hs);
         for (int i = t; i < (COUT / 8) * 128; i += kThreads) {
             const int k = i % 128, q = i / 128;
             const int64_t cell = ((int64_t)z0 * g.ny + y0 + k / 8) * g.nx + x0 + k % 8;

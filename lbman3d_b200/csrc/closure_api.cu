@@ -79,6 +79,27 @@ int resident(int threads, size_t smem) {
     return n;
 }
 
+// Resident blocks per SM of a kernel at this launch shape, from the device's
+// shared memory per SM (1 KB reserved per block), the kernel's registers and
+// static shared memory, and the thread limit.
+template <auto Kern>
+int fit_blocks(int device, int threads, size_t dyn_smem) {
+    int smem_sm = 0, regs_sm = 0, threads_sm = 0;
+    cudaFuncAttributes fa{};
+    if (cudaDeviceGetAttribute(&smem_sm, cudaDevAttrMaxSharedMemoryPerMultiprocessor, device) != cudaSuccess ||
+        cudaDeviceGetAttribute(&regs_sm, cudaDevAttrMaxRegistersPerMultiprocessor, device) != cudaSuccess ||
+        cudaDeviceGetAttribute(&threads_sm, cudaDevAttrMaxThreadsPerMultiProcessor, device) != cudaSuccess ||
+        cudaFuncGetAttributes(&fa, Kern) != cudaSuccess) {
+        cudaGetLastError();
+        return 1;
+    }
+    const size_t per_block = dyn_smem + fa.sharedSizeBytes + 1024;
+    int n = (int)((size_t)smem_sm / per_block);
+    n = std::min(n, regs_sm / std::max(1, fa.numRegs * threads));
+    n = std::min(n, threads_sm / threads);
+    return std::max(1, n);
+}
+
 }  // namespace
 
 struct lbman_closure {
@@ -104,10 +125,11 @@ struct lbman_closure {
     int* err = nullptr;
     uint32_t wait_limit = lbman::tc::kWaitLimit;  // polls of a pipeline wait before it gives up
     int Gw = 148, Gb = 296;
-    std::vector<float*> snaps;
-    std::vector<int> traj;
-    std::vector<float*> targets;
-    std::vector<int> pair_src;
+    std::vector<float*> snaps;          // filtered fine states [9V] (rho, u, Q), in recording order
+    std::vector<int> traj;              // trajectory id of each snapshot
+    std::vector<float*> targets;        // training pairs: target [8V] ...
+    std::vector<const float*> pair_in;  // ... and the input state it corrects
+    std::vector<float*> rollout_in;     // inputs of the rollout pairs (corrected-run states), owned
     int cur_traj = -1;
     float train_noise = 0.0f;  // std of N(0,1) noise on the normalised inputs in training
     float gain = 1.0f;         // correction multiplier in lbman_closure_step
@@ -120,14 +142,23 @@ int run_conv(lbman_closure* c, cudaStream_t st, const __nv_bfloat16* in, const _
              const float* bias, const __nv_bfloat16* pre_below, __nv_bfloat16* out_pre, __nv_bfloat16* out_bf,
              float* out_f) {
     if (cl::dhalo_ok(c->nx, c->ny)) {
-        constexpr size_t smem = cl::bimg_bytes(CIN, COUT) + 2 * cl::dhalo_bytes(CIN);
+        constexpr size_t smem = cl::bimg_bytes(CIN, COUT) + cl::dhalo_bytes(CIN);
         constexpr auto K = cl::conv_dhalo_kernel<CIN, COUT, MODE>;
         CL_CUDA(cudaFuncSetAttribute(K, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
-        const int64_t tiles = (int64_t)(c->nx / 8) * (c->ny / 16) * c->nz;
-        const int grid = (int)std::min<int64_t>(tiles, (int64_t)resident<K>(cl::kThreads, smem) * c->num_sms);
+        // all of the unified L1 / shared memory as shared memory: two blocks
+        // per SM
+        CL_CUDA(cudaFuncSetAttribute(K, cudaFuncAttributePreferredSharedMemoryCarveout, 100));
+        // one block per (column, z range): as many z ranges as keep every
+        // column's blocks within one wave of resident blocks (counted from
+        // the SM's shared memory, registers and threads)
+        const int cols = (c->nx / 8) * (c->ny / 16);
+        const int slots = fit_blocks<K>(c->device, cl::kZThreads, smem) * c->num_sms;
+        const int nch = std::max(1, std::min(c->nz, slots / cols));
+        const int zc = (c->nz + nch - 1) / nch;
+        const int grid = cols * ((c->nz + zc - 1) / zc);
         const cl::Grid3 gr{c->nx, c->ny, c->nz, c->V};
-        K<<<grid, cl::kThreads, smem, st>>>(gr, in, reinterpret_cast<const uint4*>(img), bias, pre_below, out_pre,
-                                            out_bf, out_f, c->err, c->wait_limit);
+        K<<<grid, cl::kZThreads, smem, st>>>(gr, zc, in, reinterpret_cast<const uint4*>(img), bias, pre_below,
+                                             out_pre, out_bf, out_f, c->err, c->wait_limit);
         CL_CUDA(cudaGetLastError());
         return LBMAN_OK;
     }
@@ -378,6 +409,7 @@ int lbman_closure_destroy(lbman_closure* c) {
     if (c->stream) cudaStreamSynchronize(c->stream);
     for (float* x : c->snaps) cudaFree(x);
     for (float* x : c->targets) cudaFree(x);
+    for (float* x : c->rollout_in) cudaFree(x);
     void* ptrs[] = {c->p, c->g, c->m, c->v, c->mask, c->act0, c->gout, c->act[0], c->act[1], c->act[2],
                     c->pre[0], c->pre[1], c->pre[2], c->gbuf[0], c->gbuf[1], c->out, c->wpart, c->bpart,
                     c->lpart, c->loss_hist, c->scales, c->err};
@@ -486,10 +518,9 @@ int lbman_closure_gradient(lbman_closure* c, const float* feat9, const float* ta
     return s == LBMAN_ERR_CUDA ? failc(s, "closure gradient failed") : s;
 }
 
-int lbman_closure_record(lbman_closure* c, lbman_solver* fine, int new_trajectory) {
-    if (!c || !fine) return failc(LBMAN_ERR_ARG, "closure: null argument");
-    SolverView v;
-    CL_TRY(solver_view(fine, &v));
+// Box-filters the fine state of v onto the coarse grid as a new snapshot of
+// trajectory `traj`.
+static int record_view(lbman_closure* c, const SolverView& v, int traj) {
     if (v.prec == LBMAN_FP64) return failc(LBMAN_ERR_UNSUPPORTED, "closure: the fine solver must be FP32 or FP16");
     if (!v.uploaded) return failc(LBMAN_ERR_STATE, "closure: fine solver has no state");
     if (v.nx % c->nx || v.ny % c->ny || v.nz % c->nz || v.nx / c->nx != v.ny / c->ny || v.nx / c->nx != v.nz / c->nz)
@@ -506,10 +537,24 @@ int lbman_closure_record(lbman_closure* c, lbman_solver* fine, int new_trajector
         cudaFree(snap);
         return cuda_fail(e, "closure record");
     }
-    if (new_trajectory || c->cur_traj < 0) ++c->cur_traj;
+    c->cur_traj = std::max(c->cur_traj, traj);
     c->snaps.push_back(snap);
-    c->traj.push_back(c->cur_traj);
+    c->traj.push_back(traj);
     return LBMAN_OK;
+}
+
+int lbman_closure_record(lbman_closure* c, lbman_solver* fine, int new_trajectory) {
+    if (!c || !fine) return failc(LBMAN_ERR_ARG, "closure: null argument");
+    SolverView v;
+    CL_TRY(solver_view(fine, &v));
+    return record_view(c, v, (new_trajectory || c->cur_traj < 0) ? c->cur_traj + 1 : c->cur_traj);
+}
+
+int lbman_closure_record_box(lbman_closure* c, lbman_ensemble* e, int box, int trajectory) {
+    if (!c || !e || trajectory < 0) return failc(LBMAN_ERR_ARG, "closure: bad arguments");
+    SolverView v;
+    CL_TRY(ensemble_box_view(e, box, &v));
+    return record_view(c, v, trajectory);
 }
 
 int lbman_closure_dataset(lbman_closure* c, int* snapshots, int* pairs) {
@@ -529,17 +574,91 @@ int lbman_closure_load_snapshot(lbman_closure* c, int k, lbman_solver* coarse) {
     return LBMAN_OK;
 }
 
+// Index of the snapshot recorded `ahead` recordings of the same trajectory
+// after snapshot k, or -1.
+static int next_of(const lbman_closure* c, int k, int ahead) {
+    int n = k;
+    for (int left = ahead; left > 0; --left) {
+        int j = n + 1;
+        while (j < (int)c->snaps.size() && c->traj[j] != c->traj[k]) ++j;
+        if (j >= (int)c->snaps.size()) return -1;
+        n = j;
+    }
+    return n;
+}
+
+// One corrected coarse step (the operator of lbman_closure_step).
+static int corrected_step(lbman_closure* c, lbman_solver* coarse) {
+    SolverView w;
+    CL_TRY(solver_view(coarse, &w));
+    CL_TRY(features(c, w.stream, static_cast<const float*>(w.rho), static_cast<const float*>(w.u),
+                    static_cast<const float*>(w.q)));
+    CL_TRY(forward(c, w.stream));
+    CL_TRY(solver_reset_populations(coarse));
+    CL_TRY(lbman_step(coarse, 1));
+    CL_TRY(solver_view(coarse, &w));
+    cl::apply_kernel<<<c->Gb, 256, 0, w.stream>>>(c->out, c->scales + 18, c->V, c->gain, static_cast<float*>(w.u),
+                                                  static_cast<float*>(w.q));
+    CL_CUDA(cudaGetLastError());
+    return LBMAN_OK;
+}
+
+int lbman_closure_add_rollout_pairs(lbman_closure* c, lbman_solver* coarse, int m, int stride, int* added) {
+    if (!c || !coarse || m < 1 || stride < 1) return failc(LBMAN_ERR_ARG, "closure: bad arguments");
+    SolverView v;
+    if (!coarse_f32(c, coarse, &v)) return failc(LBMAN_ERR_ARG, "closure: coarse solver must be FP32/FP16 on the closure grid");
+    CL_CUDA(cudaSetDevice(c->device));
+    const int64_t V = c->V;
+    int count = 0, eligible = 0;
+    for (size_t k = 0; k < c->snaps.size(); ++k) {
+        const int nk = next_of(c, (int)k, m + 1);
+        if (nk < 0 || (eligible++ % stride) != 0) continue;
+        // m corrected steps from the filtered fine state: where the corrected
+        // run actually is after m steps ...
+        const float* x = c->snaps[k];
+        CL_TRY(solver_set_state(coarse, x, x + V, x + 4 * V));
+        for (int i = 0; i < m; ++i) CL_TRY(corrected_step(c, coarse));
+        SolverView w;
+        CL_TRY(solver_view(coarse, &w));
+        float* in = nullptr;
+        CL_CUDA(cudaMalloc(&in, 9 * V * sizeof(float)));
+        c->rollout_in.push_back(in);
+        CL_CUDA(cudaMemcpyAsync(in, w.rho, V * sizeof(float), cudaMemcpyDeviceToDevice, w.stream));
+        CL_CUDA(cudaMemcpyAsync(in + V, w.u, 3 * V * sizeof(float), cudaMemcpyDeviceToDevice, w.stream));
+        CL_CUDA(cudaMemcpyAsync(in + 4 * V, w.q, 5 * V * sizeof(float), cudaMemcpyDeviceToDevice, w.stream));
+        // ... and the correction that takes its plain step to the filtered
+        // fine state one coarse step later
+        CL_TRY(solver_set_state(coarse, in, in + V, in + 4 * V));
+        CL_TRY(lbman_step(coarse, 1));
+        CL_TRY(solver_view(coarse, &w));
+        float* t = nullptr;
+        CL_CUDA(cudaMalloc(&t, 8 * V * sizeof(float)));
+        cl::target_kernel<<<c->Gb, 256, 0, w.stream>>>(c->snaps[nk], static_cast<const float*>(w.u),
+                                                        static_cast<const float*>(w.q), V, t);
+        CL_CUDA(cudaGetLastError());
+        c->targets.push_back(t);
+        c->pair_in.push_back(in);
+        ++count;
+    }
+    CL_CUDA(cudaStreamSynchronize(v.stream));
+    if (added) *added = count;
+    return check_err(c);
+}
+
 int lbman_closure_build_targets(lbman_closure* c, lbman_solver* coarse, int fit_scales) {
     if (!c || !coarse) return failc(LBMAN_ERR_ARG, "closure: null argument");
     SolverView v;
     if (!coarse_f32(c, coarse, &v)) return failc(LBMAN_ERR_ARG, "closure: coarse solver must be FP32/FP16 on the closure grid");
     CL_CUDA(cudaSetDevice(c->device));
     for (float* x : c->targets) cudaFree(x);
+    for (float* x : c->rollout_in) cudaFree(x);
     c->targets.clear();
-    c->pair_src.clear();
+    c->pair_in.clear();
+    c->rollout_in.clear();
     const int64_t V = c->V;
-    for (size_t k = 0; k + 1 < c->snaps.size(); ++k) {
-        if (c->traj[k] != c->traj[k + 1]) continue;
+    for (size_t k = 0; k < c->snaps.size(); ++k) {
+        const int nk = next_of(c, (int)k, 1);
+        if (nk < 0) continue;
         const float* x = c->snaps[k];
         CL_TRY(solver_set_state(coarse, x, x + V, x + 4 * V));
         CL_TRY(lbman_step(coarse, 1));
@@ -547,11 +666,11 @@ int lbman_closure_build_targets(lbman_closure* c, lbman_solver* coarse, int fit_
         CL_TRY(solver_view(coarse, &w));
         float* t = nullptr;
         CL_CUDA(cudaMalloc(&t, 8 * V * sizeof(float)));
-        cl::target_kernel<<<c->Gb, 256, 0, w.stream>>>(c->snaps[k + 1], static_cast<const float*>(w.u),
+        cl::target_kernel<<<c->Gb, 256, 0, w.stream>>>(c->snaps[nk], static_cast<const float*>(w.u),
                                                         static_cast<const float*>(w.q), V, t);
         CL_CUDA(cudaGetLastError());
         c->targets.push_back(t);
-        c->pair_src.push_back((int)k);
+        c->pair_in.push_back(x);
     }
     CL_CUDA(cudaStreamSynchronize(v.stream));
     if (fit_scales && !c->targets.empty()) {
@@ -620,7 +739,7 @@ int lbman_closure_train(lbman_closure* c, int iters, float lr, uint64_t seed, do
         st ^= st >> 7;
         st ^= st << 17;
         const int pi = (int)(st % (uint64_t)npairs);
-        const float* x = c->snaps[c->pair_src[pi]];
+        const float* x = c->pair_in[pi];
         CL_TRY(features(c, c->stream, x, x + V, x + 4 * V, c->train_noise, st));
         CL_TRY(forward(c, c->stream));
         CL_TRY(loss_grad(c, c->stream, c->targets[pi]));
@@ -669,19 +788,7 @@ int lbman_closure_step(lbman_closure* c, lbman_solver* coarse, int nsteps) {
     if (!coarse_f32(c, coarse, &v)) return failc(LBMAN_ERR_ARG, "closure: coarse solver must be FP32/FP16 on the closure grid");
     if (!v.uploaded) return failc(LBMAN_ERR_STATE, "closure: coarse solver has no state");
     CL_CUDA(cudaSetDevice(c->device));
-    for (int n = 0; n < nsteps; ++n) {
-        SolverView w;
-        CL_TRY(solver_view(coarse, &w));
-        CL_TRY(features(c, w.stream, static_cast<const float*>(w.rho), static_cast<const float*>(w.u),
-                        static_cast<const float*>(w.q)));
-        CL_TRY(forward(c, w.stream));
-        CL_TRY(solver_reset_populations(coarse));
-        CL_TRY(lbman_step(coarse, 1));
-        CL_TRY(solver_view(coarse, &w));
-        cl::apply_kernel<<<c->Gb, 256, 0, w.stream>>>(c->out, c->scales + 18, c->V, c->gain,
-                                                      static_cast<float*>(w.u), static_cast<float*>(w.q));
-        CL_CUDA(cudaGetLastError());
-    }
+    for (int n = 0; n < nsteps; ++n) CL_TRY(corrected_step(c, coarse));
     CL_CUDA(cudaStreamSynchronize(v.stream));
     return check_err(c);
 }

@@ -11,6 +11,7 @@
 
 #include "../../include/lbman3d.h"
 #include "ens_launch.h"
+#include "solver_view.h"
 #include "launch.h"
 #include "tiles.h"
 
@@ -190,6 +191,25 @@ int ens_build_graph(lbman_ensemble* e, int k) {
 }
 
 }  // namespace
+
+namespace lbman {
+int ensemble_box_view(lbman_ensemble* e, int box, SolverView* v) {
+    if (!e || !v || box < 0 || box >= e->n) return efail(LBMAN_ERR_ARG, "bad ensemble box");
+    const EnsBox& B = e->host[box];
+    v->prec = e->prec;
+    v->nx = B.P.nx;
+    v->ny = B.P.ny;
+    v->nz = B.P.nz;
+    v->V = B.P.V;
+    v->rho = B.rho;
+    // the velocity lives in u[0] (split) or in the buffer of the current parity (fused)
+    v->u = e->kernels == LBMAN_KERNELS_FUSED ? B.u[e->par] : B.u[0];
+    v->q = B.q[e->par];
+    v->stream = e->stream;
+    v->uploaded = e->uploaded;
+    return LBMAN_OK;
+}
+}  // namespace lbman
 
 extern "C" {
 

@@ -6,6 +6,7 @@
 #include <stdint.h>
 
 struct lbman_solver;
+struct lbman_ensemble;
 
 namespace lbman {
 
@@ -21,6 +22,9 @@ struct SolverView {
 };
 
 int solver_view(lbman_solver* s, SolverView* v);
+// The current fields of box `box` of an ensemble (rho is current after every
+// lbman_ensemble_step call).
+int ensemble_box_view(lbman_ensemble* e, int box, SolverView* v);
 // Rebuild the populations as f_eq(rho, u) of the current fields (as after an
 // upload without populations); the next step starts from them.
 int solver_reset_populations(lbman_solver* s);

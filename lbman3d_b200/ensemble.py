@@ -38,6 +38,12 @@ class Ensemble:
     def __len__(self):
         return len(self.boxes)
 
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *a):
+        self.close()
+
     def set_stream(self, stream_ptr: int):
         N.check(N.lib().lbman_ensemble_set_stream(self._h, C.c_void_p(stream_ptr)))
 

@@ -7,6 +7,7 @@ import numpy as np
 import pytest
 
 import lbman3d_b200 as L
+from lbman3d_b200 import _native as N
 from lbman3d_b200 import closure as CL
 from oracle import closure as K
 
@@ -29,9 +30,11 @@ def test_tensor_core_selftest():
     assert np.all(e >= 0) and np.all(e < 1e-6), e
 
 
-# (8, 8, 8), (5, 6, 7): gathers from global memory; (16, 16, 8), (64, 4, 4):
-# 128-cell tiles of whole x rows, staged through shared memory
-@pytest.mark.parametrize("grid", [(8, 8, 8), (5, 6, 7), (16, 16, 8), (64, 4, 4)])
+# (8, 8, 8), (5, 6, 7): gathers from global memory; (64, 4, 4): 128-cell
+# tiles of whole x rows, staged through shared memory; (16, 16, 8), (32, 64,
+# 40): the z-marching descriptor-halo kernel (one plane per block, and 16
+# columns marching 3-plane ranges with a shorter last range)
+@pytest.mark.parametrize("grid", [(8, 8, 8), (5, 6, 7), (16, 16, 8), (64, 4, 4), (32, 64, 40)])
 def test_forward_matches_oracle(grid):
     feat, _ = _case(grid, 1)
     with CL.Closure(*grid, seed=5) as cl:
@@ -67,7 +70,7 @@ def test_wait_that_gives_up_reports_timeout_and_next_call_recovers(grid):
         np.testing.assert_array_equal(g1, g0)
 
 
-@pytest.mark.parametrize("grid", [(8, 8, 8), (5, 6, 7), (16, 16, 8)])
+@pytest.mark.parametrize("grid", [(8, 8, 8), (5, 6, 7), (16, 16, 8), (32, 64, 40)])
 def test_gradient_matches_oracle(grid):
     feat, tgt = _case(grid, 2)
     with CL.Closure(*grid, seed=6) as cl:
@@ -106,6 +109,57 @@ def test_pipeline_trains_and_runs():
         cl.step(coarse, 3)
         out = coarse.download()
         assert np.all(np.isfinite(out["q"])) and np.all(np.isfinite(out["u"]))
+
+
+def test_ensemble_snapshots_and_rollout_pairs():
+    """Snapshots recorded from ensemble boxes equal those of the same runs
+    done alone; interleaved recordings pair within each trajectory; rollout
+    pairs are added from every eligible snapshot and train."""
+    fine_p = L.Params(nx=32, ny=32, nz=32, ALPHA=0.01)
+    coarse_p = CL.coarse_params(fine_p, 4)
+    S0 = L.EquilibriumScalarOrder(fine_p)
+    seeds = [3, 4]
+    with L.Ensemble([(fine_p, L.FullyPeriodicConfig())] * 2, L.Precision.FP32, N.KERNELS_SPLIT) as ens, \
+            L.Simulation(fine_p, L.FullyPeriodicConfig(), L.Precision.FP32, N.KERNELS_SPLIT, tile=(32, 6, 0)) as fine, \
+            L.Simulation(coarse_p, L.FullyPeriodicConfig(), L.Precision.FP32) as coarse, \
+            L.Simulation(coarse_p, L.FullyPeriodicConfig(), L.Precision.FP32) as probe, \
+            CL.Closure(8, 8, 8, seed=1) as cl, CL.Closure(8, 8, 8, seed=1) as ref:
+        ens.set_shape(N.KERNELS_SPLIT, 32, 6, 0)  # the single box's shape: the same arithmetic
+        ens.init_seeded_each(seeds, 1e-3)
+        ens.step(20)
+        for b in range(2):
+            cl.record_box(ens, b, b)
+        for _ in range(6):
+            ens.step(4)
+            for b in range(2):
+                cl.record_box(ens, b, b)
+        assert cl.dataset() == (14, 0)
+        fine.init_seeded(seeds[1], S0, 1e-3)
+        fine.step(20)
+        ref.record(fine, new_trajectory=True)
+        for _ in range(6):
+            fine.step(4)
+            ref.record(fine)
+        # box 1's snapshots are the odd recordings
+        for k in range(7):
+            cl.load_snapshot(2 * k + 1, coarse)
+            ref.load_snapshot(k, probe)
+            a, b = coarse.download(), probe.download()
+            for f in ("rho", "u", "q"):
+                np.testing.assert_array_equal(a[f], b[f])
+        cl.build_targets(coarse)
+        assert cl.dataset() == (14, 12)  # 6 pairs per trajectory, none across them
+        first, last = cl.train(200, lr=1e-3, seed=2)
+        assert last < first
+        # m = 2: snapshots with a third later recording of their trajectory,
+        # 4 per trajectory, every one of them (stride 1)
+        assert cl.add_rollout_pairs(coarse, 2, 1) == 8
+        assert cl.dataset() == (14, 20)
+        # m = 3: 3 eligible per trajectory, 6 in recording order, every other one
+        assert cl.add_rollout_pairs(coarse, 3, 2) == 3
+        cl.train(100, lr=5e-4, seed=3)
+        cl.build_targets(coarse, fit_scales=False)  # clears the rollout pairs
+        assert cl.dataset() == (14, 12)
 
 
 def test_trained_closure_beats_plain_coarse_on_held_out_run():
