@@ -760,13 +760,28 @@ __global__ void __launch_bounds__(kThreads) wgrad_dhalo_kernel(Grid3 g, const __
     if (t < 32) tc::tmem_dealloc(tmem, WH::TCOLS);
 }
 
-// out[j] = sum over p < P (in order) of partials[p * n + j].
-__global__ void sum_partials_kernel(const float* __restrict__ partials, int P, int n, float* __restrict__ out) {
-    const int j = blockIdx.x * blockDim.x + threadIdx.x;
-    if (j >= n) return;
+// out[j] = sum over p < P of partials[p * n + j] in a fixed order: a block
+// takes 32 consecutive j; its warp s sums the partials p = s, s + 8, ... in
+// increasing p, then the 8 slice sums are added in increasing s.  (One
+// thread per j summing all P serially left most SMs idle.)  Launch with
+// kFoldThreads threads and ceil(n / 32) blocks.
+constexpr int kFoldThreads = 256;
+__global__ void __launch_bounds__(kFoldThreads) sum_partials_kernel(const float* __restrict__ partials, int P, int n,
+                                                                     float* __restrict__ out) {
+    __shared__ float slice[kFoldThreads / 32][32];
+    const int lane = threadIdx.x & 31, s = threadIdx.x >> 5;
+    const int j = blockIdx.x * 32 + lane;
     float acc = 0.0f;
-    for (int p = 0; p < P; ++p) acc += partials[(int64_t)p * n + j];
-    out[j] = acc;
+    if (j < n)
+        for (int p = s; p < P; p += kFoldThreads / 32) acc += partials[(int64_t)p * n + j];
+    slice[s][lane] = acc;
+    __syncthreads();
+    if (s == 0 && j < n) {
+        float t = slice[0][lane];
+#pragma unroll
+        for (int k = 1; k < kFoldThreads / 32; ++k) t += slice[k][lane];
+        out[j] = t;
+    }
 }
 
 // Bias gradient partials: per block, sum over its cells of grad[c][co].

@@ -192,7 +192,7 @@ int run_wgrad(lbman_closure* c, cudaStream_t st, const __nv_bfloat16* a, const _
     }
     CL_CUDA(cudaGetLastError());
     const int n = 27 * CIN * COUT;
-    cl::sum_partials_kernel<<<(n + 255) / 256, 256, 0, st>>>(c->wpart, c->Gw, n, c->g + w_off(layer));
+    cl::sum_partials_kernel<<<(n + 31) / 32, cl::kFoldThreads, 0, st>>>(c->wpart, c->Gw, n, c->g + w_off(layer));
     CL_CUDA(cudaGetLastError());
     return LBMAN_OK;
 }
@@ -201,7 +201,7 @@ template <int C>
 int run_bias_grad(lbman_closure* c, cudaStream_t st, const __nv_bfloat16* gr, int layer) {
     cl::bias_grad_kernel<C><<<c->Gb, cl::kThreads, 0, st>>>(gr, c->V, c->bpart);
     CL_CUDA(cudaGetLastError());
-    cl::sum_partials_kernel<<<1, 64, 0, st>>>(c->bpart, c->Gb, C, c->g + b_off(layer));
+    cl::sum_partials_kernel<<<(C + 31) / 32, cl::kFoldThreads, 0, st>>>(c->bpart, c->Gb, C, c->g + b_off(layer));
     CL_CUDA(cudaGetLastError());
     return LBMAN_OK;
 }
