@@ -219,9 +219,10 @@ int default_zchunk(int nx, int ny, int nz, int tcx, int tcy, int num_sms) {
 }
 
 // Default z-marching tile before any autotuning: the widest compiled tile
-// whose last partial tile pads x by at most 10% (wide rows keep the global
-// stores of a block in full sectors); otherwise the one with the least work
-// per output cell (threads per tile cell times the x and y padding).
+// up to 32 cells whose last partial tile pads x by at most 10% (wide rows
+// keep the global stores of a block in full sectors); otherwise the one with
+// the least work per output cell (threads per tile cell times the x and y
+// padding).
 LaunchShape default_shape(const lbman_config& c, int num_sms, const Ops& ops) {
     LaunchShape L;
     L.tile.pair = c.kernels == LBMAN_KERNELS_SPLIT_PAIR;
@@ -242,7 +243,9 @@ LaunchShape default_shape(const lbman_config& c, int num_sms, const Ops& ops) {
             const double padx = (double)((c.nx + t[0] - 1) / t[0] * t[0]) / c.nx;
             const double pady = (double)((c.ny + t[1] - 1) / t[1] * t[1]) / c.ny;
             const double cost = padx * pady * ops.qforce_threads(q) / (double)(t[0] * t[1]);
-            if (padx <= 1.10 && t[0] > best_wide) {
+            // the widest tile up to one warp per row: 64-wide rows measured
+            // slower (512^3: 5.3 ms Q stage at 64x6 against 4.4 ms at 32x8)
+            if (padx <= 1.10 && t[0] <= 32 && t[0] > best_wide) {
                 best_wide = t[0];
                 L.tile.tcx = t[0];
                 L.tile.tcy = t[1];
@@ -253,9 +256,17 @@ LaunchShape default_shape(const lbman_config& c, int num_sms, const Ops& ops) {
                 L.tile.tcy = t[1];
             }
         }
+        // among the 32-wide tiles, 32x8 (what the autotuner picks for the slit
+        // and close to its 512^3 choice)
+        const QTile q328{32, 8, 1};
+        if (L.tile.tcx == 32 && ops.qforce_smem(q328) != 0) L.tile.tcy = 8;
     }
     L.qthreads = ops.qforce_threads(L.tile);
-    L.tile.zc = c.zchunk > 0 ? c.zchunk : 0;  // 0: balanced schedule, one wave
+    // fixed z chunks giving several waves of blocks: measured on B200 the
+    // autotuner picks them over the balanced one-wave schedule on every
+    // workload (the pair kernel at 512^3: 6.7 ms balanced, 4.0 ms in 64-plane
+    // chunks), so an untuned handle starts there
+    L.tile.zc = c.zchunk > 0 ? c.zchunk : default_zchunk(c.nx, c.ny, c.nz, L.tile.tcx, L.tile.tcy, num_sms);
     L.num_sms = num_sms;
     return L;
 }
@@ -375,10 +386,19 @@ int lbman_create(const lbman_config* cfg, lbman_solver** out) {
     s->cfg = *cfg;
     s->device = cfg->device;
     s->prec = cfg->precision;
-    // Measured on B200: the split organisation (Q+force kernel, then the LBM
-    // kernel) outruns the one-kernel step for every workload and tile tried,
-    // so it is the default until lbman_autotune says otherwise.
-    s->kernels = cfg->kernels == LBMAN_KERNELS_AUTO ? LBMAN_KERNELS_SPLIT : cfg->kernels;
+    // Measured on B200: the split organisations (Q+force kernel, then the
+    // LBM kernel) outrun the one-kernel step for every workload and tile
+    // tried, and the two-points-per-thread Q kernel is the faster of the two
+    // where its 30-wide tiles pad x by at most 10% (512^3: 19.3 against 18.2
+    // GLUPS untuned); so those are the defaults until lbman_autotune says
+    // otherwise.
+    int kern = cfg->kernels;
+    if (kern == LBMAN_KERNELS_AUTO) {
+        const bool pair_fits = cfg->precision != LBMAN_FP64 && cfg->nx % 4 == 0 && cfg->tile_x == 0 &&
+                               cfg->tile_y == 0 && (double)((cfg->nx + 29) / 30 * 30) <= 1.10 * cfg->nx;
+        kern = pair_fits ? LBMAN_KERNELS_SPLIT_PAIR : LBMAN_KERNELS_SPLIT;
+    }
+    s->kernels = kern;
     s->rbytes = s->prec == LBMAN_FP64 ? 8 : 4;
     s->sbytes = s->prec == LBMAN_FP64 ? 8 : (s->prec == LBMAN_FP32 ? 4 : 2);
     auto bail = [&](int code) {
@@ -393,7 +413,9 @@ int lbman_create(const lbman_config* cfg, lbman_solver** out) {
     s->num_sms = prop.multiProcessorCount;
 
     build_sim_params(*cfg, s->P);
-    s->shape = default_shape(*cfg, s->num_sms, s->ops());
+    lbman_config resolved = *cfg;
+    resolved.kernels = kern;
+    s->shape = default_shape(resolved, s->num_sms, s->ops());
     const size_t smem = s->ops().qforce_smem(s->shape.tile);
     if (smem == 0)
         return bail(fail(LBMAN_ERR_ARG, "tile %dx%d is not compiled for this precision (compiled: 30x6, 32x6, "

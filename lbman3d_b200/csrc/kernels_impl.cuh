@@ -87,8 +87,30 @@ int qforce_threads(const QTile& T) {
     return n;
 }
 
+// Resident blocks per SM that the SM's shared memory (1 KB reserved per
+// block), registers and thread limit admit for a kernel at this shape.
+template <auto Kern>
+int fit_blocks(int threads, size_t smem) {
+    int dev = 0, smem_sm = 0, regs_sm = 0, threads_sm = 0;
+    cudaFuncAttributes fa{};
+    if (cudaGetDevice(&dev) != cudaSuccess ||
+        cudaDeviceGetAttribute(&smem_sm, cudaDevAttrMaxSharedMemoryPerMultiprocessor, dev) != cudaSuccess ||
+        cudaDeviceGetAttribute(&regs_sm, cudaDevAttrMaxRegistersPerMultiprocessor, dev) != cudaSuccess ||
+        cudaDeviceGetAttribute(&threads_sm, cudaDevAttrMaxThreadsPerMultiProcessor, dev) != cudaSuccess ||
+        cudaFuncGetAttributes(&fa, Kern) != cudaSuccess) {
+        cudaGetLastError();
+        return 1;
+    }
+    int n = (int)((size_t)smem_sm / (smem + fa.sharedSizeBytes + 1024));
+    n = std::min(n, regs_sm / std::max(1, fa.numRegs * threads));
+    n = std::min(n, threads_sm / threads);
+    return std::max(1, n);
+}
+
 // Resident blocks per SM of one kernel instantiation at its launch shape
-// (queried once; the dynamic shared-memory limit is raised by prepare()).
+// (computed once; the dynamic shared-memory limit is raised by prepare()).
+// The occupancy query and the count from the SM's resources are both taken:
+// the query has answered 1 for kernels that run two blocks per SM here.
 template <auto Kern>
 int resident_blocks(int threads, size_t smem) {
     static std::atomic<int> cached{0};
@@ -98,6 +120,7 @@ int resident_blocks(int threads, size_t smem) {
             cudaGetLastError();
             n = 1;
         }
+        n = std::max(n, fit_blocks<Kern>(threads, smem));
         cached.store(n, std::memory_order_relaxed);
     }
     return n;
