@@ -209,12 +209,14 @@ int check_launch(lbman_solver* s, cudaError_t e, const char* what) {
 }
 
 
-// z chunk giving several waves of blocks over the SMs.
+// z chunk giving several waves of blocks over the SMs, and at most 256
+// planes (1024^3: 74 ms per step in 1024-plane chunks, 66 ms in 256).
 int default_zchunk(int nx, int ny, int nz, int tcx, int tcy, int num_sms) {
     const long cols = (long)((nx + tcx - 1) / tcx) * ((ny + tcy - 1) / tcy);
     const long target = (long)num_sms * 8;
     long nchunks = (target + cols - 1) / cols;
     nchunks = std::max(1L, std::min(nchunks, (long)std::max(1, nz / 8)));
+    nchunks = std::max(nchunks, (long)((nz + 255) / 256));
     return (int)((nz + nchunks - 1) / nchunks);
 }
 
