@@ -51,6 +51,9 @@ WORKLOADS = {
     # a 512^2 x 64 slab of the precision configuration: profiler captures
     # (a few GB on the device), scaled per cell to the full box
     "periodic512x64": (512, 512, 64, "periodic", 0.01, None),
+    # the largest FP32 box one GPU holds (159 GB); run with --no-extras and a
+    # pinned --kernels/--tile (the autotuner's state snapshot does not fit)
+    "periodic1024": (1024, 1024, 1024, "periodic", 0.01, None),
 }
 SEED, S0, SIGMA = 1234, 0.5, 1e-3
 # Host bytes per cell of the reference's CPU solver: FluidFields (f, f_new,
