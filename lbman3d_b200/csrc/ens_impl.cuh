@@ -13,14 +13,24 @@ namespace {
 
 template <class R, class S, bool DEV>
 struct EnsImpl {
+    // Resident blocks per SM of the persistent Q (or fused) grid: the larger
+    // of the occupancy query and the count from the SM's resources (the query
+    // has answered low for kernels that run two blocks per SM here).
     template <class TL>
     static int occupancy(bool fused) {
         int n = 0;
         const size_t smem = TL::template smem_bytes<R>();
-        if (fused)
-            cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, ens_fused_kernel<TL, R, S, DEV, false>, TL::NT, smem);
-        else
-            cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, ens_qforce_kernel<TL, R, false>, TL::NT, smem);
+        if (fused) {
+            if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, ens_fused_kernel<TL, R, S, DEV, false>, TL::NT,
+                                                              smem) != cudaSuccess)
+                cudaGetLastError();
+            n = std::max(n, impl::fit_blocks<ens_fused_kernel<TL, R, S, DEV, false>>(TL::NT, smem));
+        } else {
+            if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, ens_qforce_kernel<TL, R, false>, TL::NT, smem) !=
+                cudaSuccess)
+                cudaGetLastError();
+            n = std::max(n, impl::fit_blocks<ens_qforce_kernel<TL, R, false>>(TL::NT, smem));
+        }
         return n;
     }
 
