@@ -52,3 +52,21 @@ def test_set_shape_rejects_uncompiled_tiles():
         s.set_shape(N.KERNELS_SPLIT, 17, 5, 8)
     s.set_shape(N.KERNELS_FUSED, 14, 14, 4)
     assert s.shape()["kernels"] == N.KERNELS_FUSED and s.shape()["threads"] == 256
+
+
+def test_untuned_defaults():
+    """The shape a handle starts with before any autotuning: the pair Q
+    kernel under LBMAN_KERNELS_AUTO where its 30-wide tiles pad x by at most
+    10% (FP32/FP16, nx a multiple of 4), else the one-point split kernel in
+    32 x 8 tiles where those fit; fixed z chunks."""
+    def shape(nx, ny, nz, prec):
+        with L.Simulation(L.Params(nx=nx, ny=ny, nz=nz), L.FullyPeriodicConfig(), prec) as s:
+            return s.shape()
+    a = shape(120, 40, 40, L.Precision.FP32)  # 4 pair tiles exactly
+    assert (a["kernels"], a["tile_x"], a["tile_y"]) == (N.KERNELS_SPLIT_PAIR, 30, 10)
+    b = shape(64, 40, 40, L.Precision.FP32)  # 30-wide tiles would pad x by 40%
+    assert (b["kernels"], b["tile_x"], b["tile_y"]) == (N.KERNELS_SPLIT, 32, 8)
+    c = shape(120, 40, 40, L.Precision.FP64)  # the pair kernel is FP32 arithmetic
+    assert (c["kernels"], c["tile_x"], c["tile_y"]) == (N.KERNELS_SPLIT, 32, 8)
+    for s in (a, b, c):
+        assert 0 < s["zchunk"] <= 40  # fixed chunks, not the balanced schedule (0)
