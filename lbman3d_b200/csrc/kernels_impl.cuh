@@ -278,6 +278,21 @@ cudaError_t lbm_aa(const SimParams& P, bool odd, bool wr, void* f, const void* F
     // none, x only (slit), x and y (channel), or any
     const int wm = (P.uper[0] ? 0 : 1) | (P.uper[2] ? 0 : 2) | (P.uper[4] ? 0 : 4);
     const bool i32 = 15 * P.V < ((int64_t)1 << 31);
+    // FP16 storage, velocity axes all periodic, nx even: two cells per thread
+    // (c0, c1 and V even, so every cell pair's slots are one aligned word)
+    if constexpr (sizeof(S) == 2 && sizeof(R) == 4) {
+        if (wm == 0 && P.nx % 2 == 0 && (reinterpret_cast<uintptr_t>(f) & 3) == 0) {
+            const unsigned nb2 = blocks_for((P.c1 - P.c0) / 2, 256);
+            if (odd) {
+                auto k = i32 ? lbm_aa_odd_h2_kernel<DEV, int> : lbm_aa_odd_h2_kernel<DEV, int64_t>;
+                k<<<nb2, 256, 0, st>>>(P, dnx, dnxy, (S*)f, (const R*)F, (R*)rho, (R*)uout, wr ? 1 : 0);
+            } else {
+                auto k = i32 ? lbm_aa_even_h2_kernel<DEV, int> : lbm_aa_even_h2_kernel<DEV, int64_t>;
+                k<<<nb2, 256, 0, st>>>(P, (S*)f, (const R*)F, (R*)rho, (R*)uout, wr ? 1 : 0);
+            }
+            return cudaGetLastError();
+        }
+    }
 #define LBMAN_AA(W, I)                                                        \
     do {                                                                      \
         if (odd) launch(lbm_aa_odd_kernel<R, S, DEV, W, I>);                  \

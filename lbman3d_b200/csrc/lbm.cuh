@@ -516,6 +516,136 @@ __global__ void __launch_bounds__(256, lbm_min_blocks<R, S, WM != 0>())
     if (write_rho_all || mv) rho_buf[c] = rho;
 }
 
+// ---- in-place streaming, FP16 storage, two cells per thread ---------------
+//
+// The one-cell FP16 kernels above are bound by instruction issue (issue
+// active 60-76%, DRAM 51-56% in a profile of a periodic 512x512x64 box).
+// These forms update the cells c and c + 1 (c even; nx even, so c, V, c0 and
+// c1 are even and each pair of slots (c, c + 1) is one aligned 4-byte word):
+// the cell position, wrap offsets and slot addresses are computed once for
+// both cells, and a population of both cells moves with one __half2 access
+// wherever their slots are adjacent -- all 15 loads and stores of the even
+// step, and the 5 directions without an x component in the odd step (the
+// other 10 go to x - 1 or x + 1, whose pair straddles a word, and stay 2-byte
+// accesses).  Velocity axes all periodic (no wall rules).  Each cell's
+// arithmetic is that of the one-cell kernels (same collide, same
+// conversions), so the result is the same bit for bit; the slots a thread
+// reads and writes are the union of its two cells' slots, so the AA pattern
+// stays race-free.  Plain loads on F: this kernel writes it.  (Device code
+// only: host C++ checks of this header skip it.)
+#if defined(__CUDACC__)
+template <bool DEV, class I>
+__global__ void __launch_bounds__(256, 3)
+    lbm_aa_even_h2_kernel(const __grid_constant__ SimParams P, __half* F, const float* __restrict__ Fb,
+                          float* __restrict__ rho_buf, float* __restrict__ uout, int write_rho_all) {
+    const I c = (I)P.c0 + 2 * ((I)blockIdx.x * (I)blockDim.x + (I)threadIdx.x);
+    if (c >= (I)P.c1) return;
+    const I V = (I)P.V;
+    const Phys<float>& K = phys_ref<float>(P);
+    __half2 w[15];
+#pragma unroll
+    for (int j = 0; j < 15; ++j) w[j] = *reinterpret_cast<const __half2*>(F + j * V + c);
+    float f[15];
+    float rho, ux, uy, uz;
+    // cell c; its post-collision values replace the low halves
+#pragma unroll
+    for (int j = 0; j < 15; ++j) f[j] = __low2float(w[j]);
+    collide<float, DEV>(K, f, __ldg(Fb + c), __ldg(Fb + V + c), __ldg(Fb + 2 * V + c), rho, ux, uy, uz);
+#pragma unroll
+    for (int j = 0; j < 15; ++j) w[j] = __halves2half2(__float2half_rn(f[j]), __high2half(w[j]));
+    uout[c] = ux;
+    uout[V + c] = uy;
+    uout[2 * V + c] = uz;
+    if (write_rho_all) rho_buf[c] = rho;
+    // cell c + 1
+    const I c1 = c + 1;
+#pragma unroll
+    for (int j = 0; j < 15; ++j) f[j] = __high2float(w[j]);
+    collide<float, DEV>(K, f, __ldg(Fb + c1), __ldg(Fb + V + c1), __ldg(Fb + 2 * V + c1), rho, ux, uy, uz);
+#pragma unroll
+    for (int j = 0; j < 15; ++j) {
+        const __half2 v = __halves2half2(__low2half(w[j]), __float2half_rn(f[j]));
+        *reinterpret_cast<__half2*>(F + opp_(j) * V + c) = v;  // f*_j into slot opp(j)
+    }
+    uout[c1] = ux;
+    uout[V + c1] = uy;
+    uout[2 * V + c1] = uz;
+    if (write_rho_all) rho_buf[c1] = rho;
+}
+
+template <bool DEV, class I>
+__global__ void __launch_bounds__(256, 3)
+    lbm_aa_odd_h2_kernel(const __grid_constant__ SimParams P, FastDiv dnx, FastDiv dnxy, __half* F,
+                         const float* __restrict__ Fb, float* __restrict__ rho_buf, float* __restrict__ uout,
+                         int write_rho_all) {
+    const I c = (I)P.c0 + 2 * ((I)blockIdx.x * (I)blockDim.x + (I)threadIdx.x);
+    if (c >= (I)P.c1) return;
+    const I V = (I)P.V;
+    const Phys<float>& K = phys_ref<float>(P);
+    CellPos q;
+    q.z = (int)fdiv((uint32_t)c, dnxy);
+    const uint32_t r = (uint32_t)((int64_t)c - (int64_t)q.z * P.nxy);
+    q.y = (int)fdiv(r, dnx);
+    q.x = (int)(r - (uint32_t)q.y * (uint32_t)P.nx);
+    const AxisOff<I> o0 = axis_off<I>(P, q);  // cell c (x even)
+    CellPos q1 = q;
+    q1.x += 1;
+    const AxisOff<I> o1 = axis_off<I>(P, q1);  // cell c + 1: only the x offsets differ
+    // gather: every load of both cells issued before the first widening;
+    // directions without an x component load both cells as one word, the
+    // others load two halves, packed into one word once all are in flight
+    __half2 w[15];
+    __half a[15], b[15];
+#pragma unroll
+    for (int j = 0; j < 15; ++j) {
+        if (ex_(j) == 0) {
+            w[j] = *reinterpret_cast<const __half2*>(F + opp_(j) * V + c + src_off<I>(o0, j));
+        } else {
+            a[j] = F[opp_(j) * V + c + src_off<I>(o0, j)];
+            b[j] = F[opp_(j) * V + c + 1 + src_off<I>(o1, j)];
+        }
+    }
+#pragma unroll
+    for (int j = 0; j < 15; ++j)
+        if (ex_(j) != 0) w[j] = __halves2half2(a[j], b[j]);
+    float f[15];
+    float rho, ux, uy, uz;
+    // cell c; the directions without an x component keep its value in the
+    // low half until cell c + 1's joins it
+#pragma unroll
+    for (int j = 0; j < 15; ++j) f[j] = __low2float(w[j]);
+    collide<float, DEV>(K, f, __ldg(Fb + c), __ldg(Fb + V + c), __ldg(Fb + 2 * V + c), rho, ux, uy, uz);
+    // scatter: f*_k to slot k of c + e_k (= c - e_opp(k))
+#pragma unroll
+    for (int k = 0; k < 15; ++k) {
+        if (ex_(k) == 0) w[k] = __halves2half2(__float2half_rn(f[k]), __high2half(w[k]));
+        else Store<__half>::st(F + k * V + c + src_off<I>(o0, opp_(k)), f[k]);
+    }
+    uout[c] = ux;
+    uout[V + c] = uy;
+    uout[2 * V + c] = uz;
+    if (write_rho_all) rho_buf[c] = rho;
+    // cell c + 1
+    const I c1 = c + 1;
+#pragma unroll
+    for (int j = 0; j < 15; ++j) f[j] = __high2float(w[j]);
+    collide<float, DEV>(K, f, __ldg(Fb + c1), __ldg(Fb + V + c1), __ldg(Fb + 2 * V + c1), rho, ux, uy, uz);
+#pragma unroll
+    for (int k = 0; k < 15; ++k) {
+        if (ex_(k) == 0) {
+            const __half2 v = __halves2half2(__low2half(w[k]), __float2half_rn(f[k]));
+            *reinterpret_cast<__half2*>(F + k * V + c + src_off<I>(o0, opp_(k))) = v;
+        } else {
+            Store<__half>::st(F + k * V + c1 + src_off<I>(o1, opp_(k)), f[k]);
+        }
+    }
+    uout[c1] = ux;
+    uout[V + c1] = uy;
+    uout[2 * V + c1] = uz;
+    if (write_rho_all) rho_buf[c1] = rho;
+}
+#endif  // __CUDACC__
+
 // Pre-collision populations of direction j from a SWAP-layout buffer (for a
 // download of f): the odd step's gather of one direction.
 template <class R, class S>

@@ -101,6 +101,27 @@ def test_fp32_slabs_equal_the_whole_box(kernels, tile, bc):
     box.close()
 
 
+@pytest.mark.parametrize("grid", [(32, 20, 14), (21, 12, 14)], ids=["two_cells", "one_cell"])
+def test_fp16_slabs_equal_the_whole_box(grid):
+    """FP16 population storage on a periodic box: slabs (in-place kernels
+    restricted to the owned planes, population halos in FP16) equal the
+    whole box bit for bit, with the two-cells-per-thread kernels (nx even)
+    and the one-cell kernels."""
+    from cases import BC
+    p = _params(grid, False, ALPHA=0.02)
+    faces = L.from_face_tuples(BC["periodic"])
+    rho, u, q = _state(grid, 11)
+    box = L.Simulation(p, faces, L.Precision.FP16, N.KERNELS_SPLIT)
+    box.upload(rho, u, q)
+    with SL.SlabBox(p, faces, L.Precision.FP16, kernels=N.KERNELS_SPLIT, planes=[(0, 6), (6, 8)]) as sb:
+        sb.upload(rho, u, q)
+        for n in (3, 4):
+            box.step(n)
+            sb.step(n)
+            _compare(sb.download(f=True), box.download(f=True), exact=True)
+    box.close()
+
+
 def test_seeded_slabs_hold_the_whole_box_field():
     grid = (16, 12, 11)
     p = _params(grid, False)
