@@ -535,7 +535,7 @@ __global__ void __launch_bounds__(256, lbm_min_blocks<R, S, WM != 0>())
 // only: host C++ checks of this header skip it.)
 #if defined(__CUDACC__)
 template <bool DEV, class I>
-__global__ void __launch_bounds__(256, 3)
+__global__ void __launch_bounds__(256, 4)
     lbm_aa_even_h2_kernel(const __grid_constant__ SimParams P, __half* F, const float* __restrict__ Fb,
                           float* __restrict__ rho_buf, float* __restrict__ uout, int write_rho_all) {
     const I c = (I)P.c0 + 2 * ((I)blockIdx.x * (I)blockDim.x + (I)threadIdx.x);
@@ -562,10 +562,16 @@ __global__ void __launch_bounds__(256, 3)
 #pragma unroll
     for (int j = 0; j < 15; ++j) f[j] = __high2float(w[j]);
     collide<float, DEV>(K, f, __ldg(Fb + c1), __ldg(Fb + V + c1), __ldg(Fb + 2 * V + c1), rho, ux, uy, uz);
+    // V through an empty asm: the 15 store addresses are formed here rather
+    // than kept live from the loads across both collisions (64 registers and
+    // 4 blocks per SM instead of 80 and 3)
+    I Vs = V;
+    if constexpr (sizeof(I) == 4) asm volatile("" : "+r"(Vs));
+    else asm volatile("" : "+l"(Vs));
 #pragma unroll
     for (int j = 0; j < 15; ++j) {
         const __half2 v = __halves2half2(__low2half(w[j]), __float2half_rn(f[j]));
-        *reinterpret_cast<__half2*>(F + opp_(j) * V + c) = v;  // f*_j into slot opp(j)
+        *reinterpret_cast<__half2*>(F + opp_(j) * Vs + c) = v;  // f*_j into slot opp(j)
     }
     uout[c1] = ux;
     uout[V + c1] = uy;
